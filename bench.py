@@ -1,0 +1,521 @@
+#!/usr/bin/env python
+"""Throughput of the batched dense-solve engine on one B200 (or N replicas).
+
+One step = every system of the workload solved / inverted once, inputs already
+resident in HBM (``value``), and the same through the C ABI with pinned host
+buffers, host<->device copies included (``e2e``).  Default workload: 8,192
+macro-atom jumping matrices of order 61 inverted (invert_matrix).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config 0|1|3|4]
+    python bench.py --impl reference ...   # the reference's CPU path, all host cores
+
+The path does not shard with an exchange step: with N > 1 (torchrun) every rank
+runs an independent replica of the workload ("replicas only", weak scaling);
+``value`` is the systems of all ranks over the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from python_b200 import workloads as wl  # noqa: E402
+
+METRIC = "batched solves/s at ≤1e-10 rel err: mixed-prec vs FP64 on B200 vs GSL CPU"
+UNIT = "systems/s"
+POP_TOL = 1e-10
+L2_BYTES = 126 * 2 ** 20
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+HBM_FALLBACK_GBS = 6650.0
+
+WORKLOADS = {
+    0: "ion-balance solve, 4096 x n=27 (config-0 generator)",
+    1: "macro-atom inverse, 8192 x n=61 (config-1 generator)",
+    3: "50k cells: 10 ion solves n in {2..27} + 1 macro inverse n~U[20,200] per cell, shuffled",
+    4: "large macro inverse, 2048 x n~U[256,1024], 10% nonzero",
+}
+
+
+# --------------------------------------------------------------- workloads --
+def make_batches(config: int):
+    if config == 0:
+        return [wl.config0()]
+    if config == 1:
+        return [wl.config1()]
+    if config == 3:
+        s, i = wl.config3()
+        return [s, i]
+    if config == 4:
+        return [wl.config4()]
+    raise SystemExit(f"unknown config {config}")
+
+
+def size_class(n: int) -> str:
+    """Mirror of the engine's bucketing (python_b200/csrc/engine.cu)."""
+    for np_ in (4, 8, 12, 16, 20, 24, 28, 32):
+        if n <= np_:
+            return f"small{np_}"
+    for p in (48, 64, 96, 128):
+        if n <= p:
+            return f"cta{p}"
+    return "global"
+
+
+def kernel_name(kind: str, cls: str, mode: str) -> str:
+    if cls.startswith("small"):
+        return ("small_mixed_solve_kernel" if (mode == "mixed" and kind == "solve") else "small_exact_kernel")
+    return "cta_exact_kernel" if cls.startswith("cta") else "global_exact_kernel"
+
+
+def subset(batch: wl.Batch, idx: np.ndarray) -> wl.Batch:
+    mats = [batch.matrix(int(s)) for s in idx]
+    if batch.kind == "solve":
+        return wl.from_matrices("solve", mats, [batch.rhs(int(s)) for s in idx])
+    return wl.from_matrices("invert", mats)
+
+
+# -------------------------------------------------------------- distributed --
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def dist_init(world: int, use_cuda: bool):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group("nccl" if use_cuda else "gloo", timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(dist, value: float, device) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None and device.type == "cuda":
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# -------------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({nm for r in rows for nm, v in zip(names, r[5:9]) if v.lower() == "active"})
+        loaded = [v for v in sm if v > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- CPU side --
+def cpu_reference_run(batch: wl.Batch, threads: int, seconds: float, seed: int = 0):
+    """Time the reference's CPU path (oracle/_ref when built, else the C
+    restatement) on a bounded sample of the batch; returns (systems/s, info)."""
+    from oracle import oracle
+    which = "ref" if oracle.available("ref") else "port"
+    kind = "reference" if which == "ref" else "port"
+    rng = np.random.default_rng(seed)
+    probe = subset(batch, rng.choice(batch.nsys, size=min(32, batch.nsys), replace=False))
+    t0 = time.perf_counter()
+    (oracle.solve if batch.kind == "solve" else oracle.invert)(probe, which, threads=1)
+    per_sys = max((time.perf_counter() - t0) / probe.nsys, 1e-7)
+    want = int(min(batch.nsys, max(threads, seconds * threads / per_sys)))
+    idx = np.sort(rng.choice(batch.nsys, size=want, replace=False))
+    sample = subset(batch, idx)
+    t0 = time.perf_counter()
+    (oracle.solve if batch.kind == "solve" else oracle.invert)(sample, which, threads=threads)
+    dt = time.perf_counter() - t0
+    info = {"kind": kind, "cores": threads,
+            "sample": f"{sample.nsys} of {batch.nsys} systems (random, seeded), {dt:.1f} s wall, "
+                      f"{threads} pthreads, one serial {'solve_matrix' if batch.kind == 'solve' else 'invert_matrix'} "
+                      f"call per system on a fresh copy of A"}
+    return sample.nsys / dt, info
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    batches = make_batches(args.config)
+    threads = oracle.host_threads()
+    per_step = max(1.0, args.ref_seconds / (args.steps + args.warmup) / len(batches))
+    for _ in range(args.warmup):
+        for b in batches:
+            cpu_reference_run(b, threads, per_step * 0.25)
+    rates, infos = [], []
+    for k in range(args.steps):
+        t_sys = 0.0
+        for j, b in enumerate(batches):
+            r, info = cpu_reference_run(b, threads, per_step, seed=k * 7 + j)
+            t_sys += b.nsys / r
+            infos.append(info)
+        rates.append(sum(b.nsys for b in batches) / t_sys)
+    value = statistics.median(rates)
+    info = dict(infos[-1])
+    info["value"] = value
+    info["unit"] = UNIT
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(b.nsys for b in batches) / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators with the reference's structure)",
+            "config": {"workload": WORKLOADS[args.config], "config_index": args.config},
+            "cpu_baseline": info,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU side --
+def measured_peaks():
+    if PEAKS_FILE.exists():
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d.get("hbm_gbs", HBM_FALLBACK_GBS)), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def fp64_peak_tflops(device) -> float:
+    """cuBLAS DGEMM throughput on this GPU (8192^3), the FP64 denominator."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def accuracy(batch, out_np, status_np, mode, sample=512, seed=1):
+    """Error of the timed outputs against the CPU oracle on a sample."""
+    from oracle import oracle
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(batch.nsys, size=min(sample, batch.nsys), replace=False))
+    sub = subset(batch, idx)
+    if batch.kind == "solve":
+        xr, sr = oracle.solve(sub, "port", threads=oracle.host_threads())
+        worst, codes = 0.0, True
+        for j, s in enumerate(idx):
+            codes &= int(status_np[s]) == int(sr[j])
+            if sr[j] == 4:
+                continue
+            n, o = int(batch.n[s]), int(batch.offv[s])
+            r = xr[sub.offv[j]:sub.offv[j] + n]
+            v = out_np[o:o + n]
+            sig = np.abs(r) > 1e-20 * np.abs(r).sum()
+            if sig.any():
+                worst = max(worst, float(np.max(np.abs(v[sig] - r[sig]) / np.abs(r[sig]))))
+        return worst, bool(codes), "populations above 1e-20 of each system's total, max relative error"
+    ir, sr = oracle.invert(sub, "port", threads=oracle.host_threads())
+    worst, codes = 0.0, True
+    for j, s in enumerate(idx):
+        codes &= int(status_np[s]) == int(sr[j])
+        if sr[j] != 0:
+            continue
+        n, o = int(batch.n[s]), int(batch.offA[s])
+        r = ir[sub.offA[j]:sub.offA[j] + n * n]
+        v = out_np[o:o + n * n]
+        worst = max(worst, float(np.max(np.abs(v - r)) / np.max(np.abs(r))))
+    return worst, bool(codes), "inverse, max |X - X_ref| / max |X_ref| per matrix"
+
+
+def run_ours(args):
+    import torch
+
+    from python_b200 import engine
+    rank, world, local = dist_env()
+    dist = dist_init(world, True)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    lib = engine.load()
+    assert lib.cusolver_create() == 0, engine.last_error()
+
+    batches = make_batches(args.config)
+    modes = []
+    for b in batches:
+        if args.mode == "auto":
+            modes.append("mixed" if b.kind == "solve" else "fp64")
+        else:
+            modes.append(args.mode)
+    code = {"fp64": engine.FP64, "mixed": engine.MIXED}
+    plans, bufs = [], []
+    for b, m in zip(batches, modes):
+        plans.append(engine.Plan(b, code[m]))
+        A = torch.from_numpy(b.A).to(device)
+        out = torch.empty(b.b.size if b.kind == "solve" else b.A.size, dtype=torch.float64, device=device)
+        st = torch.full((b.nsys,), -1, dtype=torch.int32, device=device)
+        diag = torch.zeros((b.nsys,), dtype=torch.int32, device=device)
+        bb = torch.from_numpy(b.b).to(device) if b.kind == "solve" else None
+        bufs.append((A, bb, out, st, diag))
+    stream = torch.cuda.current_stream(device)
+    in_bytes = sum(b.A.nbytes + (b.b.nbytes if b.kind == "solve" else 0) for b in batches)
+
+    def step():
+        for p, (A, bb, out, st, diag) in zip(plans, bufs):
+            p.execute(A, out, st, b=bb, diag=diag, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(device)
+    barrier(dist, device)
+    clocks = ClockSampler(local).start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    barrier(dist, device)
+    clock_info = clocks.stop()
+    t_local = e0.elapsed_time(e1) / 1e3
+    t = reduce_max(dist, t_local, device)
+    nsys_step = sum(b.nsys for b in batches)
+    value = world * nsys_step * args.steps / t
+    launches = sum(p.launches for p in plans) * args.steps
+
+    # ---- accuracy of what was timed ------------------------------------
+    acc = []
+    for b, m, (A, bb, out, st, diag) in zip(batches, modes, bufs):
+        err, codes_ok, what = accuracy(b, out.cpu().numpy(), st.cpu().numpy(), m)
+        d = diag.cpu().numpy()
+        acc.append({"kind": b.kind, "mode": m, "max_rel_err": err, "codes_match": codes_ok, "measure": what,
+                    "fallback_frac": float(np.mean((d & (1 << 8)) != 0)) if m == "mixed" else 0.0})
+
+    # ---- dominant kernel: the size class with the most flops, timed alone --
+    best = None
+    for b, m in zip(batches, modes):
+        classes = np.array([size_class(int(n)) for n in b.n])
+        for c in np.unique(classes):
+            idx = np.nonzero(classes == c)[0]
+            nn = b.n[idx].astype(np.float64)
+            fl = float(np.sum(2.0 / 3.0 * nn ** 3 + 2 * nn ** 2 if b.kind == "solve" else 2.0 * nn ** 3))
+            if best is None or fl > best[0]:
+                best = (fl, b, m, c, idx)
+    fl, db, dm, dc, didx = best
+    dom = db if didx.size == db.nsys else subset(db, didx)
+    dplan = engine.Plan(dom, code[dm])
+    dA = torch.from_numpy(dom.A).to(device)
+    dout = torch.empty(dom.b.size if dom.kind == "solve" else dom.A.size, dtype=torch.float64, device=device)
+    dst = torch.empty((dom.nsys,), dtype=torch.int32, device=device)
+    dbb = torch.from_numpy(dom.b).to(device) if dom.kind == "solve" else None
+    for _ in range(3):
+        dplan.execute(dA, dout, dst, b=dbb, stream=stream)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device) \
+        if dom.A.nbytes < 2 * L2_BYTES else None
+    times = []
+    for _ in range(max(3, args.steps)):
+        if flush is not None:
+            flush.zero_()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        dplan.execute(dA, dout, dst, b=dbb, stream=stream)
+        k1.record(stream)
+        torch.cuda.synchronize(device)
+        times.append(k0.elapsed_time(k1) / 1e3)
+    t_kernel = statistics.median(times)
+    alg_bytes = dom.bytes()
+    alg_flops = dom.flops()
+    hbm_peak, peak_src = measured_peaks()
+    fp64_peak = fp64_peak_tflops(device)
+    roofline = {"bound": "hbm", "achieved": alg_bytes / t_kernel / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": alg_bytes / t_kernel / 1e9 / hbm_peak, "traffic": args.traffic,
+                "kernel": kernel_name(dom.kind, dc, dm), "size_class": dc, "launch_s": t_kernel,
+                "bytes_per_launch": alg_bytes, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
+    t_roof = max(alg_bytes / (hbm_peak * 1e9), alg_flops / (fp64_peak * 1e12))
+    roofline_fp64 = {"bound": "fp64", "achieved": alg_flops / t_kernel / 1e12, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": alg_flops / t_kernel / 1e12 / fp64_peak,
+                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul",
+                     "roofline_time_s": t_roof, "roofline_time_frac": t_roof / t_kernel,
+                     "flops_per_launch": alg_flops}
+    dplan.close()
+    del flush
+
+    # ---- end to end through the C ABI with pinned host buffers ------------
+    e2e = None
+    if not args.no_e2e:
+        host = []
+        for b in batches:
+            hA = torch.from_numpy(b.A).pin_memory().numpy()
+            hb = torch.from_numpy(b.b).pin_memory().numpy() if b.kind == "solve" else None
+            hout = torch.empty(b.b.size if b.kind == "solve" else b.A.size, dtype=torch.float64).pin_memory().numpy()
+            hst = torch.empty(b.nsys, dtype=torch.int32).pin_memory().numpy()
+            hb_batch = wl.Batch(b.kind, b.n, b.offA, hA, b.offv, hb)
+            host.append((hb_batch, hout, hst))
+        h2d = sum(hb.A.nbytes + (hb.b.nbytes if hb.kind == "solve" else 0) for hb, _, _ in host)
+        d2h = sum(ho.nbytes + hs.nbytes for _, ho, hs in host)
+
+        def e2e_step():
+            for (hb, hout, hst), m in zip(host, modes):
+                eng_mode = code[m]
+                if hb.kind == "solve":
+                    _, st_ = engine.solve_batched(hb, eng_mode, x=hout)
+                else:
+                    _, st_ = engine.invert_batched(hb, eng_mode, out=hout)
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        torch.cuda.synchronize(device)
+        barrier(dist, device)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize(device)
+        te = reduce_max(dist, time.perf_counter() - t0, device)
+        barrier(dist, device)
+        e2e = {"value": world * nsys_step * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "path": "solve_matrix_batched / invert_matrix_batched with pinned host buffers, wall clock"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle
+        threads = oracle.host_threads()
+        t_sys, infos = 0.0, []
+        for b in batches:
+            r, info = cpu_reference_run(b, threads, args.cpu_seconds / len(batches))
+            t_sys += b.nsys / r
+            infos.append(info)
+        cpu = dict(infos[0])
+        if len(infos) > 1:
+            cpu["sample"] = " + ".join(i["sample"] for i in infos)
+        cpu["value"] = nsys_step / t_sys
+        cpu["unit"] = UNIT
+
+    # plain FP64 batched kernel on the same workload, for the mixed-vs-FP64 ratio
+    fp64_value = None
+    if any(m == "mixed" for m in modes):
+        fplans = [engine.Plan(b, engine.FP64) for b in batches]
+        for _ in range(2):
+            for p, (A, bb, out, st, diag) in zip(fplans, bufs):
+                p.execute(A, out, st, b=bb, stream=stream)
+        torch.cuda.synchronize(device)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            for p, (A, bb, out, st, diag) in zip(fplans, bufs):
+                p.execute(A, out, st, b=bb, stream=stream)
+        f1.record(stream)
+        torch.cuda.synchronize(device)
+        tf = reduce_max(dist, f0.elapsed_time(f1) / 1e3, device)
+        fp64_value = world * nsys_step * args.steps / tf
+        for p in fplans:
+            p.close()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if all(m == "fp64" for m in modes) else "f32+f64",
+                "data": "synthetic (seeded generators with the reference's structure)",
+                "config": {"workload": WORKLOADS[args.config], "config_index": args.config,
+                           "systems_per_step": nsys_step, "modes": modes,
+                           "l2": (f"inputs {in_bytes / 2**20:.0f} MiB > 126 MiB L2" if in_bytes > L2_BYTES
+                                  else f"inputs {in_bytes / 2**20:.0f} MiB < L2: not flushed between steps"),
+                           "parallelism": f"replicas x{world}"},
+                "accuracy": acc, "plain_fp64_value": fp64_value,
+                "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
+                "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clock_info}
+        print(json.dumps(line), flush=True)
+    for p in plans:
+        p.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=1, choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", choices=["auto", "fp64", "mixed"], default="auto")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=120.0)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per launch of the dominant kernel from an ncu capture")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

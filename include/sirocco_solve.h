@@ -1,0 +1,115 @@
+/*
+ * sirocco_solve.h -- C ABI of the B200 batched dense-solve engine.
+ *
+ * Part 1 is a link-compatible drop-in for the reference's linear-algebra layer:
+ * the same prototypes, row-major double layout, size argument and return codes
+ * as the reference's GSL build (source/templates.h:358-360, implemented in
+ * source/matrix_cpu.c) plus the lifecycle names of its optional CUDA build
+ * (source/matrix_gpu.h:16-24).  Part 2 adds batched entry points that take a
+ * whole cycle's systems in one call.
+ *
+ * Return codes (the reference's GSL build, source/matrix_cpu.c):
+ *   solve : 0 ok; 4 singular (an exact zero on the diagonal of U, lu.c:540);
+ *           2 / 3 the first row failing the relative / absolute residual check
+ *           (matrix_cpu.c:162-187), x still written.
+ *   invert: 0 ok; 1 singular (GSL_EDOM); 8 out of memory (GSL_ENOMEM).
+ * The FP64 kernels reproduce GSL's factorisation bit for bit, so the codes match
+ * the reference's exactly; the mixed-precision mode re-runs any system whose
+ * code could differ in exact FP64.
+ */
+#ifndef SIROCCO_SOLVE_H
+#define SIROCCO_SOLVE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- part 1 -- */
+
+/* Replaces solve_matrix (source/matrix_cpu.c:310, prototype templates.h:359).
+   Solves A x = b for one n x n row-major system in host memory.  a_matrix is
+   read only (the reference factorises it in place; callers free it right
+   after).  x_matrix is written unless the code is 4.  nplasma is only used in
+   messages, as in the reference. */
+int solve_matrix(double *a_matrix, double *b_matrix, int size, double *x_matrix, int nplasma);
+
+/* Replaces invert_matrix (source/matrix_cpu.c:338, prototype templates.h:360).
+   inverted_matrix is written only when the return code is 0. */
+int invert_matrix(double *matrix, double *inverted_matrix, int num_rows);
+
+/* Replaces get_matrix_error_string (source/matrix_cpu.c:274): the text of a
+   solve_matrix code, as the reference's GSL build words it. */
+const char *get_matrix_error_string(int error_code);
+
+/* Replace the lifecycle hooks of the reference's CUDA build
+   (source/matrix_gpu.cu:125 cusolver_create, :159 cusolver_destroy, :50
+   cusolver_get_error_string).  create is idempotent and binds the calling
+   thread to the current CUDA device; destroy is a no-op when nothing was
+   created.  Both return 0 on success, else a CUDA error code. */
+int cusolver_create(void);
+int cusolver_destroy(void);
+const char *cusolver_get_error_string(int error);
+
+/* Aliases of solve_matrix / invert_matrix under the names of the reference's
+   CUDA build (source/matrix_gpu.cu:264, :332; matrix_gpu.h:20-21). */
+int gpu_solve_matrix(double *a_matrix, double *b_vector, int size, double *x_vector);
+int gpu_invert_matrix(double *matrix, double *inverse, int num_rows);
+
+/* ---------------------------------------------------------------- part 2 -- */
+
+/* Precision modes of the batched entry points. */
+#define SIROCCO_FP64 0   /* GSL-exact FP64 factorisation                         */
+#define SIROCCO_MIXED 1  /* equilibrated FP32 factorisation + FP64 refinement,
+                            exact FP64 for any system whose result or code the
+                            refinement cannot vouch for                          */
+
+/* Library error codes returned by the batched entry points (per-system codes
+   go to status[]); positive values are CUDA error codes. */
+#define SIROCCO_OK 0
+#define SIROCCO_EINVAL (-1)   /* bad argument: nsys < 0, n < 1, null pointer   */
+#define SIROCCO_ESIZE (-2)    /* a system larger than the engine supports      */
+#define SIROCCO_EMODE (-3)    /* unknown precision mode                        */
+#define SIROCCO_MAX_N 1480  /* shared-memory bound of the n > 128 path */
+
+/* Batched solve, called once per ionisation cycle (or once per n_e round of
+   the lock-step ion iteration) over all cells' systems.  The layout arrays
+   n[nsys], offA[nsys] (element offset of each matrix in A) and offv[nsys]
+   (element offset of each right-hand side in b and solution in x) are HOST
+   arrays; A, b, x and status may all be host or all be device pointers.
+   Returns 0, a negative library code, or a CUDA error code; status[s] holds the
+   reference code of system s.  For a singular system x is left unspecified. */
+int solve_matrix_batched(int nsys, const int *n, const int64_t *offA, const double *A,
+                         const int64_t *offv, const double *b, double *x, int *status);
+
+/* Batched inverse, called once per cycle from the matom-matrix cell loop. */
+int invert_matrix_batched(int nsys, const int *n, const int64_t *offA, const double *A,
+                          double *Ainv, int *status);
+
+/* Precision mode used by the two batched calls above (default SIROCCO_FP64). */
+int sirocco_set_precision(int mode);
+
+/* Plans: the size bucketing of one batch layout, its device-side copy and a
+   captured launch sequence, reusable every cycle.  kind 0 = solve, 1 = invert.
+   Layout arrays are host arrays (offv ignored for kind 1). */
+typedef struct sirocco_plan sirocco_plan;
+int sirocco_plan_create(sirocco_plan **plan, int kind, int nsys, const int *n, const int64_t *offA,
+                        const int64_t *offv, int mode);
+/* Enqueue the whole batch on `stream` (a cudaStream_t, 0 = legacy default).
+   All pointers are device pointers; b is ignored for an inverse; diag may be
+   null (bits 0-7: refinement iterations, 8: exact FP64 fallback taken). */
+int sirocco_plan_execute(sirocco_plan *plan, const double *A, const double *b, double *out,
+                         int *status, int *diag, void *stream);
+/* Number of kernel launches one execute issues. */
+int sirocco_plan_launches(const sirocco_plan *plan);
+int sirocco_plan_destroy(sirocco_plan *plan);
+
+/* Text of the last library error on this thread. */
+const char *sirocco_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIROCCO_SOLVE_H */

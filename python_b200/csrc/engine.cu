@@ -1,0 +1,631 @@
+// Host runtime and C ABI of the batched dense-solve engine.
+//
+// A plan groups the systems of one batch layout into size buckets, each served
+// by one kernel family (kernels_small.cuh for n <= 32, kernels_cta.cuh for
+// n <= 128, kernels_global.cuh above), keeps the layout on the device, and
+// launches the buckets on forked streams so small and large systems overlap.
+// The drop-in entry points (solve_matrix, invert_matrix) and the host-pointer
+// batched calls run through a per-thread context that caches plans and
+// grow-only device staging buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sirocco_solve.h"
+#include "kernels_cta.cuh"
+#include "kernels_global.cuh"
+#include "kernels_mixed.cuh"
+#include "kernels_small.cuh"
+
+namespace ss {
+
+// ------------------------------------------------------------------ errors --
+static thread_local std::string g_last_error;
+
+static void set_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+#define SS_CUDA(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      set_error("CUDA error %d (%s) at %s:%d", int(e_), cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return int(e_);                                                                       \
+    }                                                                                       \
+  } while (0)
+
+// ---------------------------------------------------------------- kernels --
+enum Family : int { kFamSmall = 0, kFamCta = 1, kFamGlobal = 2 };
+
+struct KernelSpec {
+  const void* fn = nullptr;
+  int threads = 0;
+  size_t dyn_smem = 0;
+  int sys_per_block = 1;
+  int blocks_per_sm = 1;
+};
+
+// size classes of the small family (padded row length NP, lanes per system G)
+static const int kSmallNP[] = {4, 8, 12, 16, 20, 24, 28, 32};
+static const int kCtaP[] = {48, 64, 96, 128};
+
+static int small_class(int n) {
+  for (int i = 0; i < 8; ++i)
+    if (n <= kSmallNP[i]) return i;
+  return -1;
+}
+static int cta_class(int n) {
+  for (int i = 0; i < 4; ++i)
+    if (n <= kCtaP[i]) return i;
+  return -1;
+}
+
+template <int KIND>
+static KernelSpec small_spec(int cls, int mode) {
+  KernelSpec k;
+  k.threads = kSmallThreads;
+#define SS_SMALL(I, NP, G)                                                              \
+  case I:                                                                               \
+    k.fn = (mode == SIROCCO_MIXED && KIND == kSolve)                                    \
+               ? reinterpret_cast<const void*>(&small_mixed_solve_kernel<NP, G>)        \
+               : reinterpret_cast<const void*>(&small_exact_kernel<KIND, NP, G>);       \
+    k.sys_per_block = kSmallThreads / G;                                                \
+    break;
+  switch (cls) {
+    SS_SMALL(0, 4, 4)
+    SS_SMALL(1, 8, 8)
+    SS_SMALL(2, 12, 16)
+    SS_SMALL(3, 16, 16)
+    SS_SMALL(4, 20, 32)
+    SS_SMALL(5, 24, 32)
+    SS_SMALL(6, 28, 32)
+    SS_SMALL(7, 32, 32)
+    default: break;
+  }
+#undef SS_SMALL
+  return k;
+}
+
+template <int KIND>
+static KernelSpec cta_spec(int cls) {
+  KernelSpec k;
+#define SS_CTA(I, TR, TC, RB, CB)                                                       \
+  case I:                                                                               \
+    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, TR, TC, RB, CB>);      \
+    k.threads = TR * TC;                                                                \
+    k.dyn_smem = CtaShape<KIND, TR, TC, RB, CB>::dyn_smem;                              \
+    break;
+  switch (cls) {
+    SS_CTA(0, 16, 16, 3, 3)
+    SS_CTA(1, 16, 16, 4, 4)
+    SS_CTA(2, 16, 16, 6, 6)
+    SS_CTA(3, 16, 16, 8, 8)
+    default: break;
+  }
+#undef SS_CTA
+  return k;
+}
+
+template <int KIND>
+static KernelSpec global_spec(int nmax) {
+  KernelSpec k;
+  k.fn = reinterpret_cast<const void*>(&global_exact_kernel<KIND>);
+  k.threads = kGThreads;
+  k.dyn_smem = global_smem_bytes(nmax);
+  return k;
+}
+
+static int finish_spec(KernelSpec& k) {
+  if (!k.fn) {
+    set_error("no kernel for this size class");
+    return SIROCCO_ESIZE;
+  }
+  if (k.dyn_smem > 48 * 1024)
+    SS_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k.dyn_smem)));
+  int nb = 0;
+  SS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.fn, k.threads, k.dyn_smem));
+  if (nb < 1) {
+    set_error("kernel does not fit on an SM (threads %d, shared %zu)", k.threads, k.dyn_smem);
+    return SIROCCO_ESIZE;
+  }
+  k.blocks_per_sm = nb;
+  return 0;
+}
+
+// ------------------------------------------------------------------- plans --
+struct Bucket {
+  Family fam;
+  int cls;        // size class (small / cta) or nmax (global)
+  int count;
+  int list_off;
+  KernelSpec spec;
+  int grid;
+  int64_t slab;   // global family, solve: scratch elements per CTA
+  int64_t scratch_off;
+};
+
+}  // namespace ss
+
+struct sirocco_plan {
+  int kind = 0;
+  int mode = 0;
+  int nsys = 0;
+  int device = 0;
+  int num_sms = 0;
+  int64_t totA = 0, totV = 0;
+  std::vector<ss::Bucket> buckets;
+  int* d_n = nullptr;
+  int64_t* d_offA = nullptr;
+  int64_t* d_offv = nullptr;
+  int* d_list = nullptr;
+  double* d_scratch = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev;
+  cudaEvent_t ev_fork = nullptr;
+};
+
+namespace ss {
+
+static void plan_free(sirocco_plan* p) {
+  if (!p) return;
+  cudaFree(p->d_n);
+  cudaFree(p->d_offA);
+  cudaFree(p->d_offv);
+  cudaFree(p->d_list);
+  cudaFree(p->d_scratch);
+  for (auto s : p->side) cudaStreamDestroy(s);
+  for (auto e : p->ev) cudaEventDestroy(e);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  delete p;
+}
+
+static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, const int64_t* offA,
+                      const int64_t* offv, int mode) {
+  *out = nullptr;
+  if (nsys < 0 || (nsys > 0 && (!n || !offA || (kind == kSolve && !offv)))) {
+    set_error("invalid plan arguments");
+    return SIROCCO_EINVAL;
+  }
+  if (kind != kSolve && kind != kInvert) {
+    set_error("kind must be 0 (solve) or 1 (invert)");
+    return SIROCCO_EINVAL;
+  }
+  if (mode != SIROCCO_FP64 && mode != SIROCCO_MIXED) {
+    set_error("unknown precision mode %d", mode);
+    return SIROCCO_EMODE;
+  }
+  std::unique_ptr<sirocco_plan, void (*)(sirocco_plan*)> p(new sirocco_plan(), plan_free);
+  p->kind = kind;
+  p->mode = mode;
+  p->nsys = nsys;
+  SS_CUDA(cudaGetDevice(&p->device));
+  SS_CUDA(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device));
+
+  // bucket the systems: key = (family, class); global family sorted by size
+  std::vector<int> small_l[8], cta_l[4], glob_l;
+  for (int s = 0; s < nsys; ++s) {
+    const int ns = n[s];
+    if (ns < 1 || ns > SIROCCO_MAX_N) {
+      set_error("system %d has order %d (supported 1..%d)", s, ns, SIROCCO_MAX_N);
+      return ns < 1 ? SIROCCO_EINVAL : SIROCCO_ESIZE;
+    }
+    p->totA = std::max<int64_t>(p->totA, offA[s] + int64_t(ns) * ns);
+    if (kind == kSolve) p->totV = std::max<int64_t>(p->totV, offv[s] + ns);
+    int c;
+    if ((c = small_class(ns)) >= 0) small_l[c].push_back(s);
+    else if ((c = cta_class(ns)) >= 0) cta_l[c].push_back(s);
+    else glob_l.push_back(s);
+  }
+  // largest systems first within the global bucket (longest jobs start first)
+  std::stable_sort(glob_l.begin(), glob_l.end(), [&](int x, int y) { return n[x] > n[y]; });
+
+  std::vector<int> list;
+  list.reserve(nsys);
+  int64_t scratch_elems = 0;
+  auto add_bucket = [&](Family fam, int cls, const std::vector<int>& l) -> int {
+    if (l.empty()) return 0;
+    Bucket b{};
+    b.fam = fam;
+    b.cls = cls;
+    b.count = int(l.size());
+    b.list_off = int(list.size());
+    list.insert(list.end(), l.begin(), l.end());
+    if (fam == kFamSmall) b.spec = (kind == kSolve) ? small_spec<kSolve>(cls, mode) : small_spec<kInvert>(cls, mode);
+    else if (fam == kFamCta) b.spec = (kind == kSolve) ? cta_spec<kSolve>(cls) : cta_spec<kInvert>(cls);
+    else b.spec = (kind == kSolve) ? global_spec<kSolve>(cls) : global_spec<kInvert>(cls);
+    int rc = finish_spec(b.spec);
+    if (rc) return rc;
+    const int blocks_needed = (b.count + b.spec.sys_per_block - 1) / b.spec.sys_per_block;
+    b.grid = std::max(1, std::min(blocks_needed, b.spec.blocks_per_sm * p->num_sms));
+    if (fam == kFamGlobal && kind == kSolve) {
+      b.slab = (int64_t(cls) * cls + 31) / 32 * 32;
+      b.scratch_off = scratch_elems;
+      scratch_elems += b.slab * b.grid;
+    }
+    p->buckets.push_back(b);
+    return 0;
+  };
+  int rc = 0;
+  if (!glob_l.empty() && (rc = add_bucket(kFamGlobal, n[glob_l.front()], glob_l))) return rc;
+  for (int c = 3; c >= 0; --c)
+    if ((rc = add_bucket(kFamCta, c, cta_l[c]))) return rc;
+  for (int c = 7; c >= 0; --c)
+    if ((rc = add_bucket(kFamSmall, c, small_l[c]))) return rc;
+
+  if (nsys > 0) {
+    SS_CUDA(cudaMalloc(&p->d_n, sizeof(int) * nsys));
+    SS_CUDA(cudaMalloc(&p->d_offA, sizeof(int64_t) * nsys));
+    SS_CUDA(cudaMalloc(&p->d_list, sizeof(int) * nsys));
+    SS_CUDA(cudaMemcpy(p->d_n, n, sizeof(int) * nsys, cudaMemcpyHostToDevice));
+    SS_CUDA(cudaMemcpy(p->d_offA, offA, sizeof(int64_t) * nsys, cudaMemcpyHostToDevice));
+    SS_CUDA(cudaMemcpy(p->d_list, list.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice));
+    if (kind == kSolve) {
+      SS_CUDA(cudaMalloc(&p->d_offv, sizeof(int64_t) * nsys));
+      SS_CUDA(cudaMemcpy(p->d_offv, offv, sizeof(int64_t) * nsys, cudaMemcpyHostToDevice));
+    }
+  }
+  if (scratch_elems > 0) SS_CUDA(cudaMalloc(&p->d_scratch, sizeof(double) * scratch_elems));
+  // one side stream per bucket beyond the first
+  for (size_t i = 1; i < p->buckets.size(); ++i) {
+    cudaStream_t st;
+    SS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    p->side.push_back(st);
+    cudaEvent_t e;
+    SS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p->ev.push_back(e);
+  }
+  SS_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+  *out = p.release();
+  return 0;
+}
+
+static int launch_bucket(const sirocco_plan* p, const Bucket& b, const double* A, const double* bvec,
+                         double* out, int* status, int* diag, cudaStream_t st) {
+  BatchView v;
+  v.n = p->d_n;
+  v.offA = p->d_offA;
+  v.offv = p->d_offv;
+  v.A = A;
+  v.b = bvec;
+  v.out = out;
+  v.status = status;
+  v.diag = diag;
+  v.list = p->d_list + b.list_off;
+  v.count = b.count;
+  if (b.fam == kFamGlobal) {
+    int nmax = b.cls;
+    double* scratch = p->d_scratch ? p->d_scratch + b.scratch_off : nullptr;
+    int64_t slab = b.slab;
+    void* args[] = {&v, &nmax, &scratch, &slab};
+    SS_CUDA(cudaLaunchKernel(b.spec.fn, dim3(b.grid), dim3(b.spec.threads), args, b.spec.dyn_smem, st));
+  } else if (b.fam == kFamSmall && p->mode == SIROCCO_MIXED && p->kind == kSolve) {
+    MixedParams mp = default_mixed_params();
+    void* args[] = {&v, &mp};
+    SS_CUDA(cudaLaunchKernel(b.spec.fn, dim3(b.grid), dim3(b.spec.threads), args, b.spec.dyn_smem, st));
+  } else {
+    void* args[] = {&v};
+    SS_CUDA(cudaLaunchKernel(b.spec.fn, dim3(b.grid), dim3(b.spec.threads), args, b.spec.dyn_smem, st));
+  }
+  return 0;
+}
+
+static int plan_run(sirocco_plan* p, const double* A, const double* bvec, double* out, int* status,
+                    int* diag, cudaStream_t st) {
+  if (p->buckets.empty()) return 0;
+  if (p->buckets.size() == 1) return launch_bucket(p, p->buckets[0], A, bvec, out, status, diag, st);
+  SS_CUDA(cudaEventRecord(p->ev_fork, st));
+  for (size_t i = 1; i < p->buckets.size(); ++i) SS_CUDA(cudaStreamWaitEvent(p->side[i - 1], p->ev_fork, 0));
+  int rc = launch_bucket(p, p->buckets[0], A, bvec, out, status, diag, st);
+  if (rc) return rc;
+  for (size_t i = 1; i < p->buckets.size(); ++i) {
+    rc = launch_bucket(p, p->buckets[i], A, bvec, out, status, diag, p->side[i - 1]);
+    if (rc) return rc;
+    SS_CUDA(cudaEventRecord(p->ev[i - 1], p->side[i - 1]));
+  }
+  for (size_t i = 1; i < p->buckets.size(); ++i) SS_CUDA(cudaStreamWaitEvent(st, p->ev[i - 1], 0));
+  return 0;
+}
+
+// -------------------------------------------------------- per-thread context --
+static uint64_t layout_hash(int kind, int mode, int nsys, const int* n, const int64_t* offA, const int64_t* offv) {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t(kind) << 8) ^ (uint64_t(mode) << 16) ^ (uint64_t(nsys) << 24);
+  auto mix = [&](uint64_t x) { h ^= x + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2); };
+  for (int s = 0; s < nsys; ++s) {
+    mix(uint64_t(uint32_t(n[s])));
+    mix(uint64_t(offA[s]));
+    if (offv) mix(uint64_t(offv[s]));
+  }
+  return h;
+}
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t want) {
+    if (want <= bytes) return 0;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+      set_error("cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+      return int(e);
+    }
+    bytes = want;
+    return 0;
+  }
+  ~DevBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+};
+
+struct Context {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  std::unordered_map<uint64_t, sirocco_plan*> plans;
+  std::vector<uint64_t> plan_order;
+  DevBuf bA, bb, bx, bst;
+  int mode = SIROCCO_FP64;
+  ~Context() { release(); }
+  void release() {
+    for (auto& kv : plans) plan_free(kv.second);
+    plans.clear();
+    plan_order.clear();
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    device = -1;
+  }
+  int init() {
+    int dev = 0;
+    SS_CUDA(cudaGetDevice(&dev));
+    if (device == dev && stream) return 0;
+    release();
+    SS_CUDA(cudaSetDevice(dev));
+    SS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    device = dev;
+    return 0;
+  }
+  int get_plan(int kind, int nsys, const int* n, const int64_t* offA, const int64_t* offv, int md,
+               sirocco_plan** out) {
+    const uint64_t h = layout_hash(kind, md, nsys, n, offA, offv);
+    auto it = plans.find(h);
+    if (it != plans.end()) {
+      *out = it->second;
+      return 0;
+    }
+    int rc = plan_build(out, kind, nsys, n, offA, offv, md);
+    if (rc) return rc;
+    if (plan_order.size() >= 16) {
+      auto old = plans.find(plan_order.front());
+      if (old != plans.end()) {
+        plan_free(old->second);
+        plans.erase(old);
+      }
+      plan_order.erase(plan_order.begin());
+    }
+    plans[h] = *out;
+    plan_order.push_back(h);
+    return 0;
+  }
+};
+
+static thread_local std::unique_ptr<Context> g_ctx;
+
+static Context* ctx() {
+  if (!g_ctx) g_ctx.reset(new Context());
+  return g_ctx.get();
+}
+
+static bool is_device_ptr(const void* ptr) {
+  if (!ptr) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, const double* A,
+                       const int64_t* offv, const double* b, double* out, int* status, int md) {
+  if (nsys == 0) return 0;
+  if (nsys < 0 || !n || !offA || !A || !out || !status || (kind == kSolve && (!offv || !b))) {
+    set_error("invalid batched arguments");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  sirocco_plan* p = nullptr;
+  rc = c->get_plan(kind, nsys, n, offA, kind == kSolve ? offv : nullptr, md, &p);
+  if (rc) return rc;
+  const bool dev = is_device_ptr(A);
+  if (dev) {
+    rc = plan_run(p, A, b, out, status, nullptr, c->stream);
+    if (rc) return rc;
+    SS_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+  }
+  const size_t bytesA = sizeof(double) * size_t(p->totA);
+  const size_t bytesV = sizeof(double) * size_t(p->totV);
+  if ((rc = c->bA.ensure(bytesA)) || (rc = c->bst.ensure(sizeof(int) * size_t(nsys)))) return rc;
+  if (kind == kSolve) {
+    if ((rc = c->bb.ensure(bytesV)) || (rc = c->bx.ensure(bytesV))) return rc;
+  } else if ((rc = c->bx.ensure(bytesA))) {
+    return rc;
+  }
+  double* dA = static_cast<double*>(c->bA.ptr);
+  double* db = static_cast<double*>(c->bb.ptr);
+  double* dx = static_cast<double*>(c->bx.ptr);
+  int* dst = static_cast<int*>(c->bst.ptr);
+  SS_CUDA(cudaMemcpyAsync(dA, A, bytesA, cudaMemcpyHostToDevice, c->stream));
+  if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(db, b, bytesV, cudaMemcpyHostToDevice, c->stream));
+  rc = plan_run(p, dA, db, dx, dst, nullptr, c->stream);
+  if (rc) return rc;
+  SS_CUDA(cudaMemcpyAsync(out, dx, kind == kSolve ? bytesV : bytesA, cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaMemcpyAsync(status, dst, sizeof(int) * size_t(nsys), cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// single system through the host path, honouring the reference's "output
+// untouched on a singular matrix" behaviour
+static int run_single(int kind, double* A, const double* b, int size, double* out, int* code) {
+  if (size < 1 || !A || !out || (kind == kSolve && !b)) {
+    set_error("invalid arguments");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  const int nn[1] = {size};
+  const int64_t oa[1] = {0}, ov[1] = {0};
+  sirocco_plan* p = nullptr;
+  rc = c->get_plan(kind, 1, nn, oa, kind == kSolve ? ov : nullptr, SIROCCO_FP64, &p);
+  if (rc) return rc;
+  const size_t bytesA = sizeof(double) * size_t(size) * size;
+  const size_t bytesV = sizeof(double) * size_t(size);
+  if ((rc = c->bA.ensure(bytesA)) || (rc = c->bst.ensure(sizeof(int)))) return rc;
+  if ((rc = c->bb.ensure(bytesV)) || (rc = c->bx.ensure(kind == kSolve ? bytesV : bytesA))) return rc;
+  double* dA = static_cast<double*>(c->bA.ptr);
+  double* db = static_cast<double*>(c->bb.ptr);
+  double* dx = static_cast<double*>(c->bx.ptr);
+  int* dst = static_cast<int*>(c->bst.ptr);
+  SS_CUDA(cudaMemcpyAsync(dA, A, bytesA, cudaMemcpyHostToDevice, c->stream));
+  if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(db, b, bytesV, cudaMemcpyHostToDevice, c->stream));
+  rc = plan_run(p, dA, db, dx, dst, nullptr, c->stream);
+  if (rc) return rc;
+  SS_CUDA(cudaMemcpyAsync(code, dst, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaStreamSynchronize(c->stream));
+  const bool write = (kind == kSolve) ? (*code != kSolveSingular) : (*code == kOk);
+  if (write) SS_CUDA(cudaMemcpy(out, dx, kind == kSolve ? bytesV : bytesA, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // namespace ss
+
+// ===================================================================== C ABI ==
+using namespace ss;
+
+extern "C" {
+
+int solve_matrix(double* a_matrix, double* b_matrix, int size, double* x_matrix, int nplasma) {
+  int code = kSolveSingular;
+  const int rc = run_single(kSolve, a_matrix, b_matrix, size, x_matrix, &code);
+  if (rc) {
+    // an engine failure leaves the caller's x untouched and reports the one
+    // code whose caller action is "keep the old populations" (matrix_ion.c:287-291)
+    fprintf(stderr, "solve_matrix: engine failure for plasma cell %d: %s\n", nplasma, g_last_error.c_str());
+    return kSolveSingular;
+  }
+  return code;
+}
+
+int invert_matrix(double* matrix, double* inverted_matrix, int num_rows) {
+  int code = kInvertSingular;
+  const int rc = run_single(kInvert, matrix, nullptr, num_rows, inverted_matrix, &code);
+  if (rc) {
+    fprintf(stderr, "invert_matrix: engine failure: %s\n", g_last_error.c_str());
+    return rc == int(cudaErrorMemoryAllocation) ? 8 /* GSL_ENOMEM */ : kInvertSingular;
+  }
+  return code;
+}
+
+const char* get_matrix_error_string(int error_code) {
+  // the wording of the reference's GSL build (matrix_cpu.c:59-72)
+  switch (error_code) {
+    case 2: return "some matrix rows failing relative error check";
+    case 3: return "some matrix rows failing absolute error check";
+    case 4: return "Unsolvable matrix! Determinant is zero. Defaulting to no change";
+    default: return "bad return from solve_matrix";
+  }
+}
+
+int cusolver_create(void) { return ctx()->init(); }
+
+int cusolver_destroy(void) {
+  if (g_ctx) g_ctx->release();
+  return 0;
+}
+
+const char* cusolver_get_error_string(int error) {
+  switch (error) {
+    case 0: return "The operation completed successfully";
+    case 1: return "The matrix is singular";
+    case 2: return "Some matrix rows fail the relative residual check";
+    case 3: return "Some matrix rows fail the absolute residual check";
+    case 4: return "Unsolvable matrix: a pivot is exactly zero";
+    case 8: return "Device memory allocation failed";
+    default: return "There was an unknown failure";
+  }
+}
+
+int gpu_solve_matrix(double* a_matrix, double* b_vector, int size, double* x_vector) {
+  return solve_matrix(a_matrix, b_vector, size, x_vector, -1);
+}
+
+int gpu_invert_matrix(double* matrix, double* inverse, int num_rows) {
+  return invert_matrix(matrix, inverse, num_rows);
+}
+
+int solve_matrix_batched(int nsys, const int* n, const int64_t* offA, const double* A, const int64_t* offv,
+                         const double* b, double* x, int* status) {
+  return run_batched(kSolve, nsys, n, offA, A, offv, b, x, status, ctx()->mode);
+}
+
+int invert_matrix_batched(int nsys, const int* n, const int64_t* offA, const double* A, double* Ainv,
+                          int* status) {
+  return run_batched(kInvert, nsys, n, offA, A, nullptr, nullptr, Ainv, status, ctx()->mode);
+}
+
+int sirocco_set_precision(int mode) {
+  if (mode != SIROCCO_FP64 && mode != SIROCCO_MIXED) {
+    set_error("unknown precision mode %d", mode);
+    return SIROCCO_EMODE;
+  }
+  ctx()->mode = mode;
+  return 0;
+}
+
+int sirocco_plan_create(sirocco_plan** plan, int kind, int nsys, const int* n, const int64_t* offA,
+                        const int64_t* offv, int mode) {
+  if (!plan) {
+    set_error("null plan pointer");
+    return SIROCCO_EINVAL;
+  }
+  return plan_build(plan, kind, nsys, n, offA, offv, mode);
+}
+
+int sirocco_plan_execute(sirocco_plan* plan, const double* A, const double* b, double* out, int* status,
+                         int* diag, void* stream) {
+  if (!plan || (plan->nsys > 0 && (!A || !out || !status || (plan->kind == kSolve && !b)))) {
+    set_error("invalid execute arguments");
+    return SIROCCO_EINVAL;
+  }
+  return plan_run(plan, A, b, out, status, diag, static_cast<cudaStream_t>(stream));
+}
+
+int sirocco_plan_launches(const sirocco_plan* plan) { return plan ? int(plan->buckets.size()) : 0; }
+
+int sirocco_plan_destroy(sirocco_plan* plan) {
+  plan_free(plan);
+  return 0;
+}
+
+const char* sirocco_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,240 @@
+// Mixed-precision solve for n <= 32: equilibrated FP32 LU + FP64 iterative
+// refinement, with the GSL-exact FP64 solve (kernels_small.cuh) as the
+// fallback run in place by the same lane group.
+//
+//   1. R, C = powers of two that bring every row and then every column of A to
+//      a maximum in [0.5, 1); As = fl32(R A C) (scaling by powers of two is exact).
+//   2. FP32 LU of As with partial pivoting (rows stay in their lanes).
+//   3. x0 = C As^-1 R b, then x += C As^-1 R (b - A x) with the residual in FP64
+//      on the original A, until every significant component (|x_j| above
+//      `floor` times the sum of |x|) moves by at most tol * |x_j|.
+//   4. The FP64 path re-solves the system when: the FP32 factorisation meets a
+//      zero / non-finite pivot or a pivot ratio below 1 / cond_limit (condition
+//      estimate), the refinement contracts by less than 2x per step or runs out
+//      of iterations, or the reference's own residual test (matrix_cpu.c:162-187)
+//      could land within a factor 256 n u of its 1e-6 threshold for this x, in
+//      which case only the exact FP64 solution can decide codes 2 / 3.
+// Everything that reaches the caller from the FP32 path therefore has status 0,
+// exactly as the reference would report.
+#pragma once
+#include "kernels_small.cuh"
+
+namespace ss {
+
+__host__ __device__ inline MixedParams default_mixed_params() {
+  MixedParams p;
+  p.max_iter = 12;
+  p.tol = 4.0e-16;
+  p.cond_limit = 1.0e7;
+  p.resid_margin = 1.0e-8;
+  return p;
+}
+
+// power of two 2^-e with m * 2^-e in [0.5, 1); 1 for zero / non-finite m
+__device__ __forceinline__ double pow2_inv_scale(double m) {
+  if (!(m > 0.0) || !isfinite(m)) return 1.0;
+  int e;
+  frexp(m, &e);
+  return ldexp(1.0, -e);
+}
+
+template <int NP, int G>
+__global__ void __launch_bounds__(kSmallThreads)
+small_mixed_solve_kernel(BatchView bv, MixedParams mp) {
+  constexpr int GPB = kSmallThreads / G;
+  constexpr int S = SmallSmem<NP>::S;
+  constexpr double kFloor = 1.0e-22;          // significance floor of a component (x_j / sum |x|)
+  __shared__ __align__(16) SmallSmem<NP> smem_all[GPB];
+
+  const int grp = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const unsigned gmask = group_mask<G>();
+  SmallSmem<NP>& sm = smem_all[grp];
+
+  for (int item = blockIdx.x * GPB + grp; item < bv.count; item += gridDim.x * GPB) {
+    const int s = bv.list[item];
+    const int n = bv.n[s];
+    const int64_t ov = bv.offv[s];
+    const double* __restrict__ bg = bv.b + ov;
+    double* __restrict__ xg = bv.out + ov;
+    small_stage<NP, G>(sm, bv.A + bv.offA[s], n, lane, gmask);
+    const bool act = lane < n;
+
+    // ---- 1. equilibration -------------------------------------------------
+    double rmax = 0.0;
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < NP; ++k)
+        if (k < n) rmax = fmax(rmax, fabs(sm.stage[lane * S + k]));
+    }
+    const double rs = pow2_inv_scale(rmax);
+    if (act) sm.rsc[lane] = rs;
+    __syncwarp(gmask);
+    double cmax = 0.0;
+    if (act) {
+      for (int r = 0; r < n; ++r) cmax = fmax(cmax, fabs(sm.stage[r * S + lane]) * sm.rsc[r]);
+    }
+    const double cs_own = pow2_inv_scale(cmax);
+    if (act) sm.csc[lane] = cs_own;
+    __syncwarp(gmask);
+    float af[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+      af[k] = (act && k < n) ? float(sm.stage[lane * S + k] * rs * sm.csc[k]) : 0.0f;
+
+    // ---- 2. FP32 LU, rows stay in lanes; pstep = step that chose this row --
+    bool done = false, bad = false;
+    int pstep = 0x7fff;
+    float prinv = 0.0f;
+    float umax = 0.0f, umin = 3.0e38f;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      if (j < n && !bad) {
+        float key = (act && !done) ? fabsf(af[j]) : -1.0f;
+        if (!(key == key)) key = 0.0f;
+        int kl = lane;
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) {
+          const float ok = __shfl_xor_sync(gmask, key, off, G);
+          const int ol = __shfl_xor_sync(gmask, kl, off, G);
+          if (ok > key || (ok == key && ol < kl)) { key = ok; kl = ol; }
+        }
+        if (!(key > 0.0f) || !isfinite(key)) {
+          bad = true;
+        } else {
+          umax = fmaxf(umax, key);
+          umin = fminf(umin, key);
+          const bool was_done = done;
+          if (lane == kl) {
+            done = true;
+            pstep = j;
+#pragma unroll
+            for (int k = j; k < NP; ++k) sm.fpiv[k] = af[k];
+          }
+          __syncwarp(gmask);
+          const float rinv = 1.0f / sm.fpiv[j];
+          if (lane == kl) prinv = rinv;
+          if (act && !was_done && lane != kl) {
+            const float l = af[j] * rinv;
+            af[j] = l;
+#pragma unroll
+            for (int k = j + 1; k < NP; ++k) af[k] = fmaf(-l, sm.fpiv[k], af[k]);
+          }
+          __syncwarp(gmask);
+        }
+      }
+    }
+    bool fallback = bad || (double(umin) * mp.cond_limit < double(umax));
+    int iters = 0;
+    int diagbits = 0;
+    if (bad || fallback) diagbits |= kDiagIllCond;
+
+    if (!fallback) {
+      if (act) sm.lop[pstep] = lane;
+      __syncwarp(gmask);
+      // correction: returns, in lane j, the component j of C As^-1 R v
+      auto correct = [&](double v) -> double {
+        const double w = v * rs;
+        double wmax = act ? fabs(w) : 0.0;
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) wmax = fmax(wmax, __shfl_xor_sync(gmask, wmax, off, G));
+        const double sc = pow2_inv_scale(wmax);
+        float t = act ? float(w * sc) : 0.0f;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          if (j < n) {
+            const float yj = __shfl_sync(gmask, t, sm.lop[j], G);
+            if (act && pstep > j) t = fmaf(-af[j], yj, t);
+          }
+        }
+        double dj = 0.0;
+#pragma unroll
+        for (int j = NP - 1; j >= 0; --j) {
+          if (j < n) {
+            const float zl = t * prinv;
+            const float zj = __shfl_sync(gmask, zl, sm.lop[j], G);
+            if (act && pstep < j) t = fmaf(-af[j], zj, t);
+            if (lane == j) dj = double(zj);
+          }
+        }
+        return act ? dj * sm.csc[lane] / sc : 0.0;
+      };
+
+      double xj = correct(act ? bg[lane] : 0.0);
+      double dprev = 0.0;
+      bool conv = false;
+      for (int it = 0; it < mp.max_iter; ++it) {
+        if (act) sm.xs[lane] = xj;
+        __syncwarp(gmask);
+        double res = 0.0;
+        if (act) {
+          res = bg[lane];
+#pragma unroll
+          for (int k = 0; k < NP; ++k)
+            if (k < n) res = fma(-sm.stage[lane * S + k], sm.xs[k], res);
+        }
+        __syncwarp(gmask);
+        const double d = correct(res);
+        xj += d;
+        iters = it + 1;
+        // significance-weighted size of the step
+        double ax = act ? fabs(xj) : 0.0, sx = ax, dn = act ? fabs(d) : 0.0;
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) sx += __shfl_xor_sync(gmask, sx, off, G);
+        double rel = (act && ax > kFloor * sx) ? dn / ax : 0.0;
+        double dmax = dn;
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) {
+          rel = fmax(rel, __shfl_xor_sync(gmask, rel, off, G));
+          dmax = fmax(dmax, __shfl_xor_sync(gmask, dmax, off, G));
+        }
+        if (!(rel == rel) || !(dmax == dmax)) break;     // non-finite: let FP64 decide
+        if (rel <= mp.tol) { conv = true; break; }
+        if (it > 0 && dmax > 0.5 * dprev) break;         // contraction too slow: stalled
+        dprev = dmax;
+      }
+      if (!conv) {
+        fallback = true;
+        diagbits |= kDiagNoConverge;
+      } else {
+        if (act) sm.xs[lane] = xj;
+        __syncwarp(gmask);
+        double worst;
+        const int code = small_residual_code<NP, G>(sm, bg, n, lane, gmask, &worst);
+        // how close could the reference's own residual test come to 1e-6?
+        double risk = 0.0;
+        if (act) {
+          double sabs = 0.0, y = 0.0;
+#pragma unroll
+          for (int k = 0; k < NP; ++k)
+            if (k < n) {
+              sabs = fma(fabs(sm.stage[lane * S + k]), fabs(sm.xs[k]), sabs);
+              y = fma(sm.stage[lane * S + k], sm.xs[k], y);
+            }
+          const double bound = 256.0 * n * 1.1102230246251565e-16 * sabs;
+          risk = (bg[lane] > 0.0) ? bound / fabs(y) : bound;
+          if (!(risk == risk)) risk = 1.0e300;
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) risk = fmax(risk, __shfl_xor_sync(gmask, risk, off, G));
+        if (code != 0 || worst > mp.resid_margin || risk > 0.5 * kResidEps) fallback = true;
+      }
+    }
+
+    int code;
+    if (fallback) {
+      code = small_exact_solve<NP, G>(sm, bg, xg, n, lane, gmask);
+      diagbits |= kDiagFallback;
+    } else {
+      for (int k = lane; k < n; k += G) xg[k] = sm.xs[k];
+      code = kOk;
+    }
+    if (lane == 0) {
+      bv.status[s] = code;
+      if (bv.diag) bv.diag[s] = diagbits | (iters & kDiagIterMask);
+    }
+    __syncwarp(gmask);
+  }
+}
+
+}  // namespace ss

@@ -1,0 +1,203 @@
+"""ctypes binding of the engine's C ABI (``include/sirocco_solve.h``).
+
+This is the same boundary a C host links against; the Python side only moves
+numpy / torch buffers across it.  The engine library is required: importing
+this module on a machine where ``libsirocco_solve.so`` is missing raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int64, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+from .workloads import Batch
+
+LIB_PATH = Path(__file__).resolve().parent / "libsirocco_solve.so"
+
+FP64 = 0
+MIXED = 1
+SOLVE = 0
+INVERT = 1
+
+# every symbol include/sirocco_solve.h declares
+EXPORTS = (
+    "solve_matrix", "invert_matrix", "get_matrix_error_string",
+    "cusolver_create", "cusolver_destroy", "cusolver_get_error_string",
+    "gpu_solve_matrix", "gpu_invert_matrix",
+    "solve_matrix_batched", "invert_matrix_batched", "sirocco_set_precision",
+    "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
+    "sirocco_plan_destroy", "sirocco_last_error",
+)
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise EngineError(f"engine library not built: {LIB_PATH} (run python -m python_b200.build)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    dp = POINTER(c_double)
+    lib.solve_matrix.argtypes = [dp, dp, c_int, dp, c_int]
+    lib.solve_matrix.restype = c_int
+    lib.invert_matrix.argtypes = [dp, dp, c_int]
+    lib.invert_matrix.restype = c_int
+    lib.gpu_solve_matrix.argtypes = [dp, dp, c_int, dp]
+    lib.gpu_solve_matrix.restype = c_int
+    lib.gpu_invert_matrix.argtypes = [dp, dp, c_int]
+    lib.gpu_invert_matrix.restype = c_int
+    lib.get_matrix_error_string.argtypes = [c_int]
+    lib.get_matrix_error_string.restype = c_char_p
+    lib.cusolver_get_error_string.argtypes = [c_int]
+    lib.cusolver_get_error_string.restype = c_char_p
+    lib.cusolver_create.restype = c_int
+    lib.cusolver_destroy.restype = c_int
+    lib.solve_matrix_batched.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.solve_matrix_batched.restype = c_int
+    lib.invert_matrix_batched.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.invert_matrix_batched.restype = c_int
+    lib.sirocco_set_precision.argtypes = [c_int]
+    lib.sirocco_set_precision.restype = c_int
+    lib.sirocco_plan_create.argtypes = [POINTER(c_void_p), c_int, c_int, c_void_p, c_void_p, c_void_p, c_int]
+    lib.sirocco_plan_create.restype = c_int
+    lib.sirocco_plan_execute.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.sirocco_plan_execute.restype = c_int
+    lib.sirocco_plan_launches.argtypes = [c_void_p]
+    lib.sirocco_plan_launches.restype = c_int
+    lib.sirocco_plan_destroy.argtypes = [c_void_p]
+    lib.sirocco_plan_destroy.restype = c_int
+    lib.sirocco_last_error.restype = c_char_p
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().sirocco_last_error().decode()
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise EngineError(f"{what} failed with {rc}: {last_error()}")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(c_void_p)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+# --------------------------------------------------------------- drop-in ----
+def solve_matrix(a: np.ndarray, b: np.ndarray, x: np.ndarray | None = None, nplasma: int = 0):
+    """Drop-in solve_matrix on one system; returns (code, x)."""
+    lib = load()
+    a = np.ascontiguousarray(a, np.float64).copy()
+    b = np.ascontiguousarray(b, np.float64)
+    n = b.size
+    if x is None:
+        x = np.full(n, np.nan)
+    code = lib.solve_matrix(_dptr(a), _dptr(b), n, _dptr(x), nplasma)
+    return code, x
+
+
+def invert_matrix(m: np.ndarray, out: np.ndarray | None = None):
+    """Drop-in invert_matrix on one system; returns (code, inverse)."""
+    lib = load()
+    m = np.ascontiguousarray(m, np.float64).copy()
+    n = m.shape[0]
+    if out is None:
+        out = np.full((n, n), np.nan)
+    code = lib.invert_matrix(_dptr(m), _dptr(out), n)
+    return code, out
+
+
+def error_string(code: int) -> str:
+    return load().get_matrix_error_string(code).decode()
+
+
+# --------------------------------------------------------------- batched ----
+def set_precision(mode: int) -> None:
+    _check(load().sirocco_set_precision(mode), "sirocco_set_precision")
+
+
+def solve_batched(batch: Batch, mode: int = FP64, x: np.ndarray | None = None):
+    """Host-buffer batched solve through solve_matrix_batched; returns (x, status)."""
+    lib = load()
+    set_precision(mode)
+    n = np.ascontiguousarray(batch.n, np.int32)
+    if x is None:
+        x = np.full(batch.b.size, np.nan)
+    st = np.full(batch.nsys, -99, np.int32)
+    rc = lib.solve_matrix_batched(batch.nsys, _ptr(n), _ptr(batch.offA), _ptr(batch.A), _ptr(batch.offv),
+                                  _ptr(batch.b), _ptr(x), _ptr(st))
+    _check(rc, "solve_matrix_batched")
+    return x, st
+
+
+def invert_batched(batch: Batch, mode: int = FP64, out: np.ndarray | None = None):
+    """Host-buffer batched inverse through invert_matrix_batched; returns (inverses, status)."""
+    lib = load()
+    set_precision(mode)
+    n = np.ascontiguousarray(batch.n, np.int32)
+    if out is None:
+        out = np.full(batch.A.size, np.nan)
+    st = np.full(batch.nsys, -99, np.int32)
+    rc = lib.invert_matrix_batched(batch.nsys, _ptr(n), _ptr(batch.offA), _ptr(batch.A), _ptr(out), _ptr(st))
+    _check(rc, "invert_matrix_batched")
+    return out, st
+
+
+class Plan:
+    """A device-resident plan (sirocco_plan_*) over one batch layout.
+
+    ``execute`` takes torch CUDA tensors (or raw device addresses) and enqueues
+    the whole batch on the given stream (default: torch's current stream).
+    """
+
+    def __init__(self, batch: Batch, mode: int = FP64):
+        lib = load()
+        self.kind = SOLVE if batch.kind == "solve" else INVERT
+        self._n = np.ascontiguousarray(batch.n, np.int32)
+        self._offA = np.ascontiguousarray(batch.offA, np.int64)
+        self._offv = np.ascontiguousarray(batch.offv if batch.offv is not None else np.zeros(batch.nsys), np.int64)
+        h = c_void_p()
+        rc = lib.sirocco_plan_create(ctypes.byref(h), self.kind, batch.nsys, _ptr(self._n), _ptr(self._offA),
+                                     _ptr(self._offv), mode)
+        _check(rc, "sirocco_plan_create")
+        self._h = h
+        self.nsys = batch.nsys
+        self.launches = lib.sirocco_plan_launches(h)
+
+    def execute(self, A, out, status, b=None, diag=None, stream=None) -> None:
+        def addr(t):
+            if t is None:
+                return None
+            return c_void_p(t if isinstance(t, int) else t.data_ptr())
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+        elif not isinstance(stream, int):
+            stream = stream.cuda_stream
+        rc = load().sirocco_plan_execute(self._h, addr(A), addr(b), addr(out), addr(status), addr(diag),
+                                         c_void_p(stream))
+        _check(rc, "sirocco_plan_execute")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().sirocco_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,199 @@
+"""Seeded synthetic batches with the shapes and value distributions of the
+per-cell systems that the reference solves.
+
+Ion-balance systems follow the rate-matrix layout that
+``populate_ion_rate_matrix`` builds (reference ``source/matrix_ion.c:445-659``):
+``A[j][k]`` is the rate from stage k to stage j, each diagonal entry is minus
+its column sum, and one row is replaced by ones with ``b`` the unit vector on
+that row (number conservation, ``matrix_ion.c:633-655``).
+
+Macro-atom systems follow ``calc_matom_matrix``
+(``source/macro_accelerate.c:269-284``): ``N = I - Q`` where each row of the
+jumping matrix ``Q`` sums to ``1 - p_deact`` and rows with no transitions are
+identity rows.
+
+All batches are float64, row-major, packed one system after another; the
+packing offsets are returned beside them (``offA`` in elements of A,
+``offv`` in elements of b / x).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+BASE_SEED = 20261203
+ION_SIZES_PER_CELL = (2, 3, 7, 8, 9, 11, 13, 15, 17, 27)
+
+
+@dataclass
+class Batch:
+    kind: str                  # "solve" or "invert"
+    n: np.ndarray              # int32 [nsys]
+    offA: np.ndarray           # int64 [nsys], element offset of each matrix
+    A: np.ndarray              # float64 [sum n^2]
+    offv: np.ndarray | None = None   # int64 [nsys], element offset of b / x
+    b: np.ndarray | None = None      # float64 [sum n]
+
+    @property
+    def nsys(self) -> int:
+        return int(self.n.size)
+
+    def matrix(self, s: int) -> np.ndarray:
+        n = int(self.n[s])
+        return self.A[self.offA[s]:self.offA[s] + n * n].reshape(n, n)
+
+    def rhs(self, s: int) -> np.ndarray:
+        n = int(self.n[s])
+        return self.b[self.offv[s]:self.offv[s] + n]
+
+    def flops(self) -> float:
+        n = self.n.astype(np.float64)
+        if self.kind == "solve":
+            return float(np.sum(2.0 / 3.0 * n ** 3 + 2.0 * n ** 2))
+        return float(np.sum(2.0 * n ** 3))
+
+    def bytes(self) -> float:
+        n = self.n.astype(np.float64)
+        if self.kind == "solve":
+            return float(np.sum(8.0 * (n ** 2 + 2 * n)))
+        return float(np.sum(16.0 * n ** 2))
+
+
+def offsets(n: np.ndarray, square: bool) -> np.ndarray:
+    sz = n.astype(np.int64) ** 2 if square else n.astype(np.int64)
+    off = np.zeros(n.size, np.int64)
+    if n.size > 1:
+        off[1:] = np.cumsum(sz[:-1])
+    return off
+
+
+def _loguniform(rng, lo, hi, size=None):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size))
+
+
+def ion_matrix(rng, n: int, spread=(1e-14, 1e2), auger=(1e-16, 1e-6),
+               auger_frac=0.1, conservation="last"):
+    """One ion-balance system of n stages (config-0 generator).
+
+    Stage k ionises to k+1 at rate I_k and k+1 recombines to k at rate R_k,
+    both log-uniform in ``spread``; a fraction ``auger_frac`` of the
+    k -> k+2..k+4 entries carry a rate log-uniform in ``auger``.
+    """
+    a = np.zeros((n, n))
+    if n > 1:
+        ion = _loguniform(rng, *spread, n - 1)
+        rec = _loguniform(rng, *spread, n - 1)
+        k = np.arange(n - 1)
+        a[k + 1, k] = ion
+        a[k, k + 1] = rec
+    for d in (2, 3, 4):
+        if n > d:
+            k = np.arange(n - d)
+            hit = rng.random(n - d) < auger_frac
+            a[k[hit] + d, k[hit]] = _loguniform(rng, *auger, int(hit.sum()))
+    a[np.diag_indices(n)] = 0.0
+    a[np.diag_indices(n)] = -a.sum(axis=0)
+    b = np.zeros(n)
+    row = n - 1 if conservation == "last" else 0
+    a[row, :] = 1.0
+    b[row] = 1.0
+    return a, b
+
+
+def macro_matrix(rng, n: int, density=0.25, qrange=(1e-8, 1.0),
+                 pdeact=(1e-4, 0.5), identity_frac=0.03):
+    """One macro-atom N = I - Q of order n (config-1 generator)."""
+    q = np.where(rng.random((n, n)) < density, _loguniform(rng, *qrange, (n, n)), 0.0)
+    q[np.diag_indices(n)] = 0.0
+    empty = rng.random(n) < identity_frac
+    q[empty] = 0.0
+    rs = q.sum(axis=1)
+    p = rng.uniform(*pdeact, n)
+    scale = np.where(rs > 0, (1.0 - p) / np.where(rs > 0, rs, 1.0), 0.0)
+    q *= scale[:, None]
+    return np.eye(n) - q
+
+
+def _pack(kind, mats, rhs=None) -> Batch:
+    n = np.array([m.shape[0] for m in mats], np.int32)
+    offA = offsets(n, True)
+    A = np.concatenate([m.ravel() for m in mats]) if mats else np.zeros(0)
+    if kind == "solve":
+        offv = offsets(n, False)
+        b = np.concatenate(rhs) if rhs else np.zeros(0)
+        return Batch(kind, n, offA, np.ascontiguousarray(A), offv, np.ascontiguousarray(b))
+    return Batch(kind, n, offA, np.ascontiguousarray(A))
+
+
+def config0(nsys=4096, n=27, seed=BASE_SEED + 0, conservation="last") -> Batch:
+    """4,096 ion-balance systems of order 27, solved (plain FP64 solve_matrix)."""
+    rng = np.random.default_rng(seed)
+    mats, rhs = [], []
+    for _ in range(nsys):
+        a, b = ion_matrix(rng, n, conservation=conservation)
+        mats.append(a)
+        rhs.append(b)
+    return _pack("solve", mats, rhs)
+
+
+def config1(nsys=8192, n=61, seed=BASE_SEED + 1) -> Batch:
+    """8,192 macro-atom matrices N = I - Q of order 61, inverted."""
+    rng = np.random.default_rng(seed)
+    return _pack("invert", [macro_matrix(rng, n) for _ in range(nsys)])
+
+
+def config3(ncells=50_000, seed=BASE_SEED + 3, macro_range=(20, 200)):
+    """Mixed-size batch: per cell 10 ion systems (orders ION_SIZES_PER_CELL)
+    and one macro-atom inverse of order uniform in ``macro_range``; the order
+    of systems is shuffled.  Returns (solve batch, invert batch)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.tile(np.array(ION_SIZES_PER_CELL), ncells)
+    rng.shuffle(sizes)
+    mats, rhs = [], []
+    for n in sizes:
+        a, b = ion_matrix(rng, int(n))
+        mats.append(a)
+        rhs.append(b)
+    msz = rng.integers(macro_range[0], macro_range[1] + 1, ncells)
+    macro = [macro_matrix(rng, int(n)) for n in msz]
+    return _pack("solve", mats, rhs), _pack("invert", macro)
+
+
+def config4(nsys=2048, seed=BASE_SEED + 4, nrange=(256, 1024)) -> Batch:
+    """Large macro atoms: orders uniform in ``nrange``, 10 % of Q nonzero."""
+    rng = np.random.default_rng(seed)
+    sz = rng.integers(nrange[0], nrange[1] + 1, nsys)
+    return _pack("invert", [macro_matrix(rng, int(n), density=0.10) for n in sz])
+
+
+def ion_batch(sizes, seed, conservation="last", spread=(1e-14, 1e2)) -> Batch:
+    rng = np.random.default_rng(seed)
+    mats, rhs = [], []
+    for n in sizes:
+        a, b = ion_matrix(rng, int(n), spread=spread, conservation=conservation)
+        mats.append(a)
+        rhs.append(b)
+    return _pack("solve", mats, rhs)
+
+
+def macro_batch(sizes, seed, density=0.25) -> Batch:
+    rng = np.random.default_rng(seed)
+    return _pack("invert", [macro_matrix(rng, int(n), density=density) for n in sizes])
+
+
+def dense_batch(kind, sizes, seed, log_spread=0.0) -> Batch:
+    """General dense systems (Gaussian entries times exp(U[-s, s]))."""
+    rng = np.random.default_rng(seed)
+    mats, rhs = [], []
+    for n in sizes:
+        n = int(n)
+        m = rng.standard_normal((n, n)) * np.exp(rng.uniform(-log_spread, log_spread, (n, n)))
+        mats.append(m)
+        rhs.append(rng.standard_normal(n))
+    return _pack(kind, mats, rhs if kind == "solve" else None)
+
+
+def from_matrices(kind, mats, rhs=None) -> Batch:
+    return _pack(kind, [np.ascontiguousarray(m, dtype=np.float64) for m in mats],
+                 [np.ascontiguousarray(r, dtype=np.float64) for r in rhs] if rhs is not None else None)

@@ -1,0 +1,162 @@
+"""Parity of the CUDA engine with the reference, through the C ABI.
+
+FP64 mode: the factorisation is GSL's bit for bit, so solutions and every
+return code must equal the reference build's exactly; inverses agree to
+rounding (GSL groups the inverse's sums recursively).
+Mixed mode: codes exactly; populations above 1e-20 of each system's total
+within 1e-10 relative; normwise backward error within n * 1e-15.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from python_b200 import workloads as wl
+from tests.helpers import (backward_err, batch_from_golden, inverse_rel_err, population_rel_err,
+                           same_values)
+
+pytestmark = pytest.mark.gpu
+
+POP_TOL = 1e-10
+
+
+def solved_mask(batch, st):
+    return np.repeat(st != 4, batch.n)
+
+
+# ------------------------------------------------------------------ FP64 ----
+def test_fp64_golden_solves_bit_exact(engine, golden_solve):
+    batch = batch_from_golden(golden_solve, "solve")
+    x, st = engine.solve_batched(batch, engine.FP64)
+    np.testing.assert_array_equal(st, golden_solve["status_ref"])
+    m = solved_mask(batch, st)
+    assert same_values(x[m], golden_solve["x_ref"][m]).all()
+
+
+def test_fp64_golden_inverses(engine, golden_invert):
+    batch = batch_from_golden(golden_invert, "invert")
+    inv, st = engine.invert_batched(batch, engine.FP64)
+    np.testing.assert_array_equal(st, golden_invert["status_ref"])
+    assert inverse_rel_err(inv, golden_invert["inv_ref"], batch.n, batch.offA, st == 0) < 1e-9
+
+
+def test_dropin_reference_fixtures(engine, golden_fixtures):
+    g = golden_fixtures
+    for name in ("small_matrix", "matrix_ion"):
+        code, x = engine.solve_matrix(g[f"{name}_A"], g[f"{name}_b"])
+        assert code == g[f"{name}_code_ref"][0]
+        assert same_values(x, g[f"{name}_x_ref"]).all()
+        np.testing.assert_allclose(x, g[f"{name}_x_fixture"], rtol=1e-6, atol=1e-6)
+    for name in ("inverse_small", "inverse_macro"):
+        code, inv = engine.invert_matrix(g[f"{name}_M"])
+        assert code == g[f"{name}_code_ref"][0] == 0
+        ref = g[f"{name}_inv_ref"]
+        assert np.max(np.abs(inv - ref)) <= 1e-12 * np.max(np.abs(ref))
+        np.testing.assert_allclose(inv, g[f"{name}_inv_fixture"], rtol=2e-4, atol=1e-6)
+
+
+def test_dropin_singular_leaves_output_untouched(engine):
+    a = np.array([[1.0, 2.0], [2.0, 4.0]])
+    x0 = np.full(2, 7.0)
+    code, x = engine.solve_matrix(a, np.ones(2), x0.copy())
+    assert code == 4 and (x == x0).all()
+    code, inv = engine.invert_matrix(a, np.full((2, 2), 7.0))
+    assert code == 1 and (inv == 7.0).all()
+
+
+@pytest.mark.parametrize("sizes", [list(range(1, 33)), [33, 40, 47, 48, 50, 63, 64, 65, 80, 96, 100, 127, 128],
+                                   [129, 150, 178, 200, 257]])
+def test_fp64_every_size_class_matches_oracle(engine, sizes):
+    rng = np.random.default_rng(sum(sizes))
+    reps = 3 if max(sizes) <= 128 else 1
+    szs = [n for n in sizes for _ in range(reps)]
+    batch = wl.dense_batch("solve", szs, seed=int(rng.integers(1 << 30)), log_spread=4.0)
+    x, st = engine.solve_batched(batch, engine.FP64)
+    xr, sr = oracle.solve(batch, "port", threads=oracle.host_threads())
+    np.testing.assert_array_equal(st, sr)
+    m = solved_mask(batch, st)
+    assert same_values(x[m], xr[m]).all()
+    ib = wl.dense_batch("invert", szs, seed=int(rng.integers(1 << 30)))
+    inv, si = engine.invert_batched(ib, engine.FP64)
+    ir, sir = oracle.invert(ib, "port", threads=oracle.host_threads())
+    np.testing.assert_array_equal(si, sir)
+    assert inverse_rel_err(inv, ir, ib.n, ib.offA, si == 0) < 1e-9
+
+
+def test_fp64_config0_full_size_bit_exact(engine):
+    batch = wl.config0()
+    x, st = engine.solve_batched(batch, engine.FP64)
+    xr, sr = oracle.solve(batch, "port", threads=oracle.host_threads())
+    np.testing.assert_array_equal(st, sr)
+    assert same_values(x, xr).all()
+    # conservation row: populations of each system sum to 1
+    sums = np.add.reduceat(x, batch.offv.astype(np.intp))
+    assert np.max(np.abs(sums - 1.0)) < 1e-12
+
+
+def test_fp64_config1_full_size(engine):
+    batch = wl.config1()
+    inv, st = engine.invert_batched(batch, engine.FP64)
+    assert (st == 0).all()
+    sub = wl.Batch("invert", batch.n[:512], batch.offA[:512], batch.A[:batch.offA[512]])
+    ir, sr = oracle.invert(sub, "port", threads=oracle.host_threads())
+    assert inverse_rel_err(inv[:sub.A.size], ir, sub.n, sub.offA) < 1e-12
+    # size-independent checks on every system: M M^-1 = I, and the absorbing
+    # row sums of N^-1 (1 - q) = 1 for the jumping matrix N = I - Q
+    worst_id = 0.0
+    for s in range(0, batch.nsys, 97):
+        M = batch.matrix(s)
+        X = inv[batch.offA[s]:batch.offA[s] + M.size].reshape(M.shape)
+        worst_id = max(worst_id, np.max(np.abs(M @ X - np.eye(M.shape[0]))))
+        pdeact = M.sum(axis=1)                       # 1 - row sum of Q
+        np.testing.assert_allclose(X @ pdeact, np.ones(M.shape[0]), rtol=1e-10)
+    assert worst_id < 1e-10
+
+
+def test_batched_device_plan_and_graph(engine):
+    import torch
+    batch = wl.config0(nsys=1000)
+    dev = torch.device("cuda")
+    A = torch.from_numpy(batch.A).to(dev)
+    b = torch.from_numpy(batch.b).to(dev)
+    x = torch.empty_like(b)
+    st = torch.full((batch.nsys,), -1, dtype=torch.int32, device=dev)
+    plan = engine.Plan(batch, engine.FP64)
+    plan.execute(A, x, st, b=b)
+    torch.cuda.synchronize()
+    xr, sr = oracle.solve(batch, "port")
+    assert (st.cpu().numpy() == sr).all() and same_values(x.cpu().numpy(), xr).all()
+    # the same sequence captured in a CUDA graph and replayed
+    x.zero_()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            plan.execute(A, x, st, b=b, stream=s)
+    g.replay()
+    torch.cuda.synchronize()
+    assert same_values(x.cpu().numpy(), xr).all()
+    plan.close()
+
+
+# ----------------------------------------------------------------- mixed ----
+def test_mixed_golden_codes_and_values(engine, golden_solve):
+    batch = batch_from_golden(golden_solve, "solve")
+    x, st = engine.solve_batched(batch, engine.MIXED)
+    np.testing.assert_array_equal(st, golden_solve["status_ref"])
+    ok = st == 0
+    m = np.repeat(ok, batch.n)
+    sub_off = np.zeros(int(ok.sum()), np.int64)
+    sub_n = batch.n[ok]
+    sub_off[1:] = np.cumsum(sub_n[:-1])
+    assert population_rel_err(x[m], golden_solve["x_ref"][m], sub_n, sub_off) <= POP_TOL
+
+
+def test_mixed_config0_accuracy(engine):
+    batch = wl.config0()
+    x, st = engine.solve_batched(batch, engine.MIXED)
+    xr, sr = oracle.solve(batch, "port", threads=oracle.host_threads())
+    np.testing.assert_array_equal(st, sr)
+    assert population_rel_err(x, xr, batch.n, batch.offv) <= POP_TOL
+    for s in range(0, batch.nsys, 131):
+        n, o = int(batch.n[s]), int(batch.offv[s])
+        assert backward_err(batch.matrix(s), x[o:o + n], batch.rhs(s)) <= n * 1e-15
