@@ -98,7 +98,9 @@ int sirocco_plan_create(sirocco_plan **plan, int kind, int nsys, const int *n, c
                         const int64_t *offv, int mode);
 /* Enqueue the whole batch on `stream` (a cudaStream_t, 0 = legacy default).
    All pointers are device pointers; b is ignored for an inverse; diag may be
-   null (bits 0-7: refinement iterations, 8: exact FP64 fallback taken). */
+   null (bits 0-7: refinement iterations; bit 8: the result came from the
+   GSL-exact FP64 path, always so in FP64 mode; bit 9: refinement stalled;
+   bit 10: condition estimate above the mixed-mode limit). */
 int sirocco_plan_execute(sirocco_plan *plan, const double *A, const double *b, double *out,
                          int *status, int *diag, void *stream);
 /* Number of kernel launches one execute issues. */

@@ -110,9 +110,9 @@ static KernelSpec cta_spec(int cls) {
     k.dyn_smem = CtaShape<KIND, TR, TC, RB, CB>::dyn_smem;                              \
     break;
   switch (cls) {
-    SS_CTA(0, 16, 16, 3, 3)
-    SS_CTA(1, 16, 16, 4, 4)
-    SS_CTA(2, 16, 16, 6, 6)
+    SS_CTA(0, 8, 8, 6, 6)
+    SS_CTA(1, 8, 8, 8, 8)
+    SS_CTA(2, 16, 8, 6, 12)
     SS_CTA(3, 16, 16, 8, 8)
     default: break;
   }
@@ -373,11 +373,32 @@ struct DevBuf {
   }
 };
 
+// A packed host batch split into chunks of consecutive systems, each with its
+// own plan, so that the copies of one chunk overlap the kernels of another.
+struct Pipeline {
+  struct Chunk {
+    int s0, s1;
+    int64_t a0, a1, v0, v1;   // element ranges of A / out and of b / x
+    sirocco_plan* plan;
+  };
+  std::vector<Chunk> chunks;
+  ~Pipeline() {
+    for (auto& c : chunks) plan_free(c.plan);
+  }
+};
+
+constexpr int kPipeStreams = 4;
+constexpr int64_t kChunkBytes = int64_t(16) << 20;
+
 struct Context {
   int device = -1;
   cudaStream_t stream = nullptr;
+  cudaStream_t pipe[kPipeStreams] = {};
+  cudaEvent_t pipe_ev[kPipeStreams] = {};
   std::unordered_map<uint64_t, sirocco_plan*> plans;
   std::vector<uint64_t> plan_order;
+  std::unordered_map<uint64_t, std::unique_ptr<Pipeline>> pipes;
+  std::vector<uint64_t> pipe_order;
   DevBuf bA, bb, bx, bst;
   int mode = SIROCCO_FP64;
   ~Context() { release(); }
@@ -385,6 +406,14 @@ struct Context {
     for (auto& kv : plans) plan_free(kv.second);
     plans.clear();
     plan_order.clear();
+    pipes.clear();
+    pipe_order.clear();
+    for (int i = 0; i < kPipeStreams; ++i) {
+      if (pipe[i]) cudaStreamDestroy(pipe[i]);
+      if (pipe_ev[i]) cudaEventDestroy(pipe_ev[i]);
+      pipe[i] = nullptr;
+      pipe_ev[i] = nullptr;
+    }
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
     device = -1;
@@ -396,7 +425,58 @@ struct Context {
     release();
     SS_CUDA(cudaSetDevice(dev));
     SS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    for (int i = 0; i < kPipeStreams; ++i) {
+      SS_CUDA(cudaStreamCreateWithFlags(&pipe[i], cudaStreamNonBlocking));
+      SS_CUDA(cudaEventCreateWithFlags(&pipe_ev[i], cudaEventDisableTiming));
+    }
     device = dev;
+    return 0;
+  }
+  // chunked plans of a packed layout (systems stored one after another)
+  int get_pipeline(int kind, int nsys, const int* n, const int64_t* offA, const int64_t* offv, int md,
+                   Pipeline** out) {
+    const uint64_t h = layout_hash(kind, md, nsys, n, offA, offv) ^ 0x5bd1e995ull;
+    auto it = pipes.find(h);
+    if (it != pipes.end()) {
+      *out = it->second.get();
+      return 0;
+    }
+    std::unique_ptr<Pipeline> pl(new Pipeline());
+    std::vector<int64_t> ra, rv;
+    int s0 = 0;
+    while (s0 < nsys) {
+      int s1 = s0;
+      int64_t bytes = 0;
+      while (s1 < nsys && (s1 == s0 || bytes < kChunkBytes)) {
+        bytes += int64_t(n[s1]) * n[s1] * 8;
+        ++s1;
+      }
+      Pipeline::Chunk c;
+      c.s0 = s0;
+      c.s1 = s1;
+      c.a0 = offA[s0];
+      c.a1 = offA[s1 - 1] + int64_t(n[s1 - 1]) * n[s1 - 1];
+      c.v0 = offv ? offv[s0] : 0;
+      c.v1 = offv ? offv[s1 - 1] + n[s1 - 1] : 0;
+      ra.resize(s1 - s0);
+      rv.resize(s1 - s0);
+      for (int s = s0; s < s1; ++s) {
+        ra[s - s0] = offA[s] - c.a0;
+        rv[s - s0] = offv ? offv[s] - c.v0 : 0;
+      }
+      c.plan = nullptr;
+      int rc = plan_build(&c.plan, kind, s1 - s0, n + s0, ra.data(), offv ? rv.data() : nullptr, md);
+      if (rc) return rc;
+      pl->chunks.push_back(c);
+      s0 = s1;
+    }
+    if (pipe_order.size() >= 8) {
+      pipes.erase(pipe_order.front());
+      pipe_order.erase(pipe_order.begin());
+    }
+    *out = pl.get();
+    pipes[h] = std::move(pl);
+    pipe_order.push_back(h);
     return 0;
   }
   int get_plan(int kind, int nsys, const int* n, const int64_t* offA, const int64_t* offv, int md,
@@ -472,6 +552,33 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
   double* db = static_cast<double*>(c->bb.ptr);
   double* dx = static_cast<double*>(c->bx.ptr);
   int* dst = static_cast<int*>(c->bst.ptr);
+  bool packed = true;
+  for (int s = 0; s + 1 < nsys && packed; ++s) {
+    packed = offA[s + 1] == offA[s] + int64_t(n[s]) * n[s] && (kind != kSolve || offv[s + 1] == offv[s] + n[s]);
+  }
+  if (packed && bytesA > size_t(2 * kChunkBytes)) {
+    // chunked pipeline: the copies of one chunk overlap the kernels of the others
+    Pipeline* pl = nullptr;
+    rc = c->get_pipeline(kind, nsys, n, offA, kind == kSolve ? offv : nullptr, md, &pl);
+    if (rc) return rc;
+    SS_CUDA(cudaEventRecord(c->pipe_ev[0], c->stream));
+    for (int i = 0; i < kPipeStreams; ++i) SS_CUDA(cudaStreamWaitEvent(c->pipe[i], c->pipe_ev[0], 0));
+    for (size_t k = 0; k < pl->chunks.size(); ++k) {
+      const Pipeline::Chunk& ch = pl->chunks[k];
+      cudaStream_t st = c->pipe[k % kPipeStreams];
+      const size_t na = size_t(ch.a1 - ch.a0), nv = size_t(ch.v1 - ch.v0), ns = size_t(ch.s1 - ch.s0);
+      SS_CUDA(cudaMemcpyAsync(dA + ch.a0, A + ch.a0, na * sizeof(double), cudaMemcpyHostToDevice, st));
+      if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(db + ch.v0, b + ch.v0, nv * sizeof(double), cudaMemcpyHostToDevice, st));
+      double* xo = (kind == kSolve) ? dx + ch.v0 : dx + ch.a0;
+      rc = plan_run(ch.plan, dA + ch.a0, db + ch.v0, xo, dst + ch.s0, nullptr, st);
+      if (rc) return rc;
+      if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(out + ch.v0, xo, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+      else SS_CUDA(cudaMemcpyAsync(out + ch.a0, xo, na * sizeof(double), cudaMemcpyDeviceToHost, st));
+      SS_CUDA(cudaMemcpyAsync(status + ch.s0, dst + ch.s0, ns * sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
+    for (int i = 0; i < kPipeStreams; ++i) SS_CUDA(cudaStreamSynchronize(c->pipe[i]));
+    return 0;
+  }
   SS_CUDA(cudaMemcpyAsync(dA, A, bytesA, cudaMemcpyHostToDevice, c->stream));
   if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(db, b, bytesV, cudaMemcpyHostToDevice, c->stream));
   rc = plan_run(p, dA, db, dx, dst, nullptr, c->stream);

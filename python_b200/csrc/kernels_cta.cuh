@@ -2,17 +2,20 @@
 // few dozen levels, per-element macro populations).
 //
 // The padded P x P matrix lives in registers: a TR x TC thread grid where the
-// thread (tr, tc) owns rows [tr*RB, tr*RB+RB) and columns [tc*CB, tc*CB+CB).
-// Rows never move; each row carries its current position.  Step j:
+// thread (tr, tc) owns rows [tr*RB, tr*RB+RB) and columns [tc*CB, tc*CB+CB);
+// a warp covers 32/TC whole thread rows, so every thread finds the owner of
+// (its row, column j) in its own warp.  Rows never move; each row carries its
+// current position.  Step j:
 //   A  owners of column j propose their best (|a_rj|, pos) row, reduced across
 //      the owner lanes of each warp by shuffles, one candidate per warp to
 //      shared memory;                                          -- barrier
 //   B  every thread reduces the per-warp candidates (same answer everywhere),
-//      updates row positions, the pivot row's owners publish it and the
-//      column owners publish the multipliers;                 -- barrier
-//   C  every thread applies the rank-1 update to its block.
-// The column loop is split into a dynamic block loop and a static CB-wide
-// inner loop so every register index is a compile-time constant.
+//      updates row positions, takes its rows' column-j entries from the owner
+//      lane by shuffle and forms its own multipliers; the pivot row's owners
+//      publish that row;                                      -- barrier
+//   C  every thread applies the rank-1 update to its RB x CB block.
+// Register indices stay compile-time constants: the element of column j in a
+// thread's block is picked with a short predicated chain.
 //
 // Arithmetic: as in kernels_small.cuh (GSL-exact below-pivot updates; the
 // solve's triangular sweeps follow LU_svx's order, run by one warp from a
@@ -22,6 +25,15 @@
 
 namespace ss {
 
+// v[c] for a run-time c in [0, W) without dynamic register indexing
+template <int W>
+__device__ __forceinline__ double pick(const double (&v)[W], int c) {
+  double x = v[0];
+#pragma unroll
+  for (int i = 1; i < W; ++i) x = (c == i) ? v[i] : x;
+  return x;
+}
+
 template <int KIND, int TR, int TC, int RB, int CB>
 struct CtaShape {
   static constexpr int P = TR * RB;
@@ -29,20 +41,23 @@ struct CtaShape {
   static constexpr int NW = NT / 32;
   static constexpr int LS = P + 1;                          // LU row stride in shared memory
   static constexpr size_t dyn_smem = (KIND == kSolve) ? size_t(P) * LS * sizeof(double) : 0;
+  // resident CTAs per SM asked of the register allocator: about 3 registers
+  // per owned element plus a fixed ~48 for indices and the step state
+  static constexpr int regs = 48 + 3 * RB * CB;
+  static constexpr int min_blocks = (65536 / (NT * (regs > 255 ? 255 : regs))) < 1 ? 1 : (65536 / (NT * (regs > 255 ? 255 : regs)));
   static_assert(TC * CB == P, "square padding");
   static_assert(TC <= 32 && (32 % TC) == 0, "column groups tile a warp");
   static_assert(NT % 32 == 0, "whole warps");
 };
 
 template <int KIND, int TR, int TC, int RB, int CB>
-__global__ void __launch_bounds__(TR * TC, 1)
+__global__ void __launch_bounds__(TR * TC, (CtaShape<KIND, TR, TC, RB, CB>::min_blocks))
 cta_exact_kernel(BatchView bv) {
   using Sh = CtaShape<KIND, TR, TC, RB, CB>;
   constexpr int P = Sh::P;
   constexpr int NW = Sh::NW;
   constexpr int LS = Sh::LS;
 
-  __shared__ __align__(16) double lbuf[P];
   __shared__ __align__(16) double ubuf[P];
   __shared__ double ckey[NW], cval[NW];
   __shared__ int cpk[NW];
@@ -57,6 +72,7 @@ cta_exact_kernel(BatchView bv) {
   const int tr = t / TC, tc = t % TC;
   const int wid = t >> 5, wl = t & 31;
   const int row0 = tr * RB, col0 = tc * CB;
+  const int grp_lane0 = wl & ~(TC - 1);       // lane of (this thread row, tc = 0)
 
   for (int item = blockIdx.x; item < bv.count; item += gridDim.x) {
     const int s = bv.list[item];
@@ -77,129 +93,128 @@ cta_exact_kernel(BatchView bv) {
     }
     unsigned done = 0;
     bool sing = false;
-    const int nblk = (n + CB - 1) / CB;
 
-    for (int jb = 0; jb < nblk && !sing; ++jb) {
+    for (int j = 0; j < n && !sing; ++j) {
+      const int jb = j / CB, cj = j - jb * CB;
+      // ---- A: candidates of column j --------------------------------------
+      double key = -1.0, val = 0.0;
+      int pk = 0x7fffffff;                     // (pos << 16) | row
+      if (tc == jb) {
 #pragma unroll
-      for (int cj = 0; cj < CB; ++cj) {
-        const int j = jb * CB + cj;
-        if (j < n && !sing) {
-          // ---- A: candidates of column j --------------------------------
-          double key = -1.0, val = 0.0;
-          int pk = 0x7fffffff;                     // (pos << 16) | row
-          if (tc == jb) {
+        for (int r = 0; r < RB; ++r) {
+          const int row = row0 + r;
+          const double arj = pick<CB>(a[r], cj);
+          if (row < n && !((done >> r) & 1u)) {
+            const double k = pivot_key(arj);
+            const int pp = (pos[r] << 16) | row;
+            if (pivot_better(k, pp, key, pk)) { key = k; pk = pp; val = arj; }
+          }
+        }
+      }
 #pragma unroll
-            for (int r = 0; r < RB; ++r) {
-              const int row = row0 + r;
-              if (row < n && !((done >> r) & 1u)) {
-                const double k = pivot_key(a[r][cj]);
-                const int pp = (pos[r] << 16) | row;
-                if (pivot_better(k, pp, key, pk)) { key = k; pk = pp; val = a[r][cj]; }
-              }
+      for (int off = TC; off < 32; off <<= 1) {
+        const double ok = __shfl_xor_sync(0xffffffffu, key, off);
+        const double ov = __shfl_xor_sync(0xffffffffu, val, off);
+        const int op = __shfl_xor_sync(0xffffffffu, pk, off);
+        if (pivot_better(ok, op, key, pk)) { key = ok; pk = op; val = ov; }
+      }
+      if (wl == jb) { ckey[wid] = key; cval[wid] = val; cpk[wid] = pk; }
+      __syncthreads();
+
+      // ---- B: the pivot, positions, multipliers, published pivot row -------
+      key = -1.0; pk = 0x7fffffff; val = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const double k = ckey[w];
+        const int pp = cpk[w];
+        if (pivot_better(k, pp, key, pk)) { key = k; pk = pp; val = cval[w]; }
+      }
+      const int p = pk & 0xffff, ppos = pk >> 16;
+      const double ujj = val;
+      const unsigned was_done = done;
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        if (row0 + r == p) { pos[r] = j; done |= 1u << r; }
+        else if (pos[r] == j) pos[r] = ppos;
+      }
+      if (t == 0) ipiv[j] = ppos;
+      if (ujj == 0.0) {
+        sing = true;                           // uniform: every thread read the same ujj
+        continue;
+      }
+      const double rinv = __drcp_rn(ujj);      // correctly rounded, = fl(1/ujj)
+      const int prb = p / RB, prr = p - prb * RB;
+      // multipliers of this thread's rows; column j lives in lane (tr, jb)
+      double lr[RB];
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const double mine = pick<CB>(a[r], cj);
+        const double arj = __shfl_sync(0xffffffffu, mine, grp_lane0 + jb);
+        const int row = row0 + r;
+        double l = 0.0;
+        if (row < n && row != p) {
+          if (!((was_done >> r) & 1u)) l = gsl_multiplier(arj, ujj, rinv);
+          else if (KIND == kInvert) l = mul_rn(arj, rinv);
+        }
+        lr[r] = l;
+      }
+      if (tr == prb) {
+#pragma unroll
+        for (int r = 0; r < RB; ++r)
+          if (r == prr) {
+#pragma unroll
+            for (int c = 0; c < CB; ++c) ubuf[col0 + c] = a[r][c];
+          }
+      }
+      __syncthreads();
+
+      // ---- C: rank-1 update ------------------------------------------------
+      double uc[CB];
+#pragma unroll
+      for (int c = 0; c < CB; ++c) uc[c] = ubuf[col0 + c];
+      const bool own_col = (tc == jb);
+      if (KIND == kInvert) {
+        // rows whose multiplier is 0 (the pivot row, padding) keep their values
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+#pragma unroll
+          for (int c = 0; c < CB; ++c) a[r][c] = sub_rn(a[r][c], mul_rn(lr[r], uc[c]));
+        }
+        if (tr == prb) {
+#pragma unroll
+          for (int r = 0; r < RB; ++r)
+            if (r == prr) {
+#pragma unroll
+              for (int c = 0; c < CB; ++c) a[r][c] = mul_rn(a[r][c], rinv);
             }
-          }
-#pragma unroll
-          for (int off = TC; off < 32; off <<= 1) {
-            const double ok = __shfl_xor_sync(0xffffffffu, key, off);
-            const double ov = __shfl_xor_sync(0xffffffffu, val, off);
-            const int op = __shfl_xor_sync(0xffffffffu, pk, off);
-            if (pivot_better(ok, op, key, pk)) { key = ok; pk = op; val = ov; }
-          }
-          if (wl == jb) { ckey[wid] = key; cval[wid] = val; cpk[wid] = pk; }
-          __syncthreads();
-
-          // ---- B: the pivot, positions, published row and multipliers ---
-          key = -1.0; pk = 0x7fffffff; val = 0.0;
-#pragma unroll
-          for (int w = 0; w < NW; ++w) {
-            const double k = ckey[w];
-            const int pp = cpk[w];
-            if (pivot_better(k, pp, key, pk)) { key = k; pk = pp; val = cval[w]; }
-          }
-          const int p = pk & 0xffff, ppos = pk >> 16;
-          const double ujj = val;
-          const unsigned was_done = done;
+        }
+        if (own_col) {
+          // column j becomes column j of the inverse-in-place: -l, and 1/u_jj on the pivot row
 #pragma unroll
           for (int r = 0; r < RB; ++r) {
-            if (row0 + r == p) { pos[r] = j; done |= 1u << r; }
-            else if (pos[r] == j) pos[r] = ppos;
+            const double v = (row0 + r == p) ? rinv : -lr[r];
+#pragma unroll
+            for (int c = 0; c < CB; ++c)
+              if (c == cj) a[r][c] = v;
           }
-          if (t == 0) ipiv[j] = ppos;
-          if (ujj == 0.0) {
-            sing = true;
-          } else {
-            const double rinv = div_rn(1.0, ujj);
-            const int prb = p / RB, prr = p - prb * RB;
-            if (tr == prb) {
+        }
+      } else {
+        if (tc >= jb) {
 #pragma unroll
-              for (int r = 0; r < RB; ++r)
-                if (r == prr) {
+          for (int r = 0; r < RB; ++r) {
 #pragma unroll
-                  for (int c = 0; c < CB; ++c) ubuf[col0 + c] = a[r][c];
-                }
-            }
-            if (tc == jb) {
+            for (int c = 0; c < CB; ++c)
+              if (tc > jb || c > cj) a[r][c] = sub_rn(a[r][c], mul_rn(lr[r], uc[c]));
+          }
+        }
+        if (own_col) {
 #pragma unroll
-              for (int r = 0; r < RB; ++r) {
-                const int row = row0 + r;
-                double l = 0.0;
-                if (row < n && row != p) {
-                  if (!((was_done >> r) & 1u)) l = gsl_multiplier(a[r][cj], ujj, rinv);
-                  else if (KIND == kInvert) l = mul_rn(a[r][cj], rinv);
-                }
-                lbuf[row] = l;
-              }
-            }
-            __syncthreads();
-
-            // ---- C: rank-1 update ----------------------------------------
-            double lr[RB], uc[CB];
+          for (int r = 0; r < RB; ++r) {
+            const int row = row0 + r;
+            if (row < n && row != p && !((was_done >> r) & 1u)) {
 #pragma unroll
-            for (int r = 0; r < RB; ++r) lr[r] = lbuf[row0 + r];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) uc[c] = ubuf[col0 + c];
-            if (KIND == kInvert) {
-#pragma unroll
-              for (int r = 0; r < RB; ++r) {
-                if (lr[r] != 0.0) {
-#pragma unroll
-                  for (int c = 0; c < CB; ++c)
-                    if (!(tc == jb && c == cj)) a[r][c] = sub_rn(a[r][c], mul_rn(lr[r], uc[c]));
-                }
-              }
-              if (tr == prb) {
-#pragma unroll
-                for (int r = 0; r < RB; ++r)
-                  if (r == prr) {
-#pragma unroll
-                    for (int c = 0; c < CB; ++c) a[r][c] = mul_rn(a[r][c], rinv);
-                  }
-              }
-              if (tc == jb) {
-#pragma unroll
-                for (int r = 0; r < RB; ++r) {
-                  const int row = row0 + r;
-                  if (row < n) a[r][cj] = (row == p) ? rinv : -lr[r];
-                }
-              }
-            } else {
-              if (tc >= jb) {
-#pragma unroll
-                for (int r = 0; r < RB; ++r) {
-                  if (lr[r] != 0.0) {
-#pragma unroll
-                    for (int c = 0; c < CB; ++c)
-                      if (tc > jb || c > cj) a[r][c] = sub_rn(a[r][c], mul_rn(lr[r], uc[c]));
-                  }
-                }
-              }
-              if (tc == jb) {
-#pragma unroll
-                for (int r = 0; r < RB; ++r) {
-                  const int row = row0 + r;
-                  if (row < n && row != p && !((was_done >> r) & 1u)) a[r][cj] = lr[r];
-                }
-              }
+              for (int c = 0; c < CB; ++c)
+                if (c == cj) a[r][c] = lr[r];
             }
           }
         }
@@ -209,7 +224,7 @@ cta_exact_kernel(BatchView bv) {
     if (sing) {
       if (t == 0) {
         bv.status[s] = (KIND == kSolve) ? kSolveSingular : kInvertSingular;
-        if (bv.diag) bv.diag[s] = 0;
+        if (bv.diag) bv.diag[s] = kDiagExact;
       }
       __syncthreads();
       continue;
@@ -241,7 +256,7 @@ cta_exact_kernel(BatchView bv) {
       }
       if (t == 0) {
         bv.status[s] = kOk;
-        if (bv.diag) bv.diag[s] = 0;
+        if (bv.diag) bv.diag[s] = kDiagExact;
       }
     } else {
       // factors into shared memory by position; cmap[i] = original row at position i
@@ -299,7 +314,7 @@ cta_exact_kernel(BatchView bv) {
         for (int i = wl; i < n; i += 32) bv.out[ov + i] = xs[i];
         if (wl == 0) {
           bv.status[s] = fcode;
-          if (bv.diag) bv.diag[s] = 0;
+          if (bv.diag) bv.diag[s] = kDiagExact;
         }
       }
     }

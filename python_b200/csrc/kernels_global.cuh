@@ -104,7 +104,7 @@ global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
         __syncthreads();
         const double ujj = Ps[j * kGPS + k];
         if (ujj == 0.0) { sing = true; break; }
-        const double rinv = div_rn(1.0, ujj);
+        const double rinv = __drcp_rn(ujj);   // correctly rounded, = fl(1/ujj)
         double piv[kGNB];
 #pragma unroll
         for (int c = 0; c < kGNB; ++c) piv[c] = Ps[j * kGPS + c];
@@ -209,7 +209,7 @@ global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
     if (sing) {
       if (t == 0) {
         bv.status[s] = (KIND == kSolve) ? kSolveSingular : kInvertSingular;
-        if (bv.diag) bv.diag[s] = 0;
+        if (bv.diag) bv.diag[s] = kDiagExact;
       }
       __syncthreads();
       continue;
@@ -235,7 +235,7 @@ global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
       }
       if (t == 0) {
         bv.status[s] = kOk;
-        if (bv.diag) bv.diag[s] = 0;
+        if (bv.diag) bv.diag[s] = kDiagExact;
       }
     } else {
       double* vec = Ps;                 // y, then x (natural order), n doubles each
@@ -291,7 +291,7 @@ global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
         for (int i = wl; i < n; i += 32) bv.out[ov + i] = xs[i];
         if (wl == 0) {
           bv.status[s] = fcode;
-          if (bv.diag) bv.diag[s] = 0;
+          if (bv.diag) bv.diag[s] = kDiagExact;
         }
       }
     }

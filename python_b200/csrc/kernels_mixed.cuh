@@ -10,8 +10,8 @@
 //      `floor` times the sum of |x|) moves by at most tol * |x_j|.
 //   4. The FP64 path re-solves the system when: the FP32 factorisation meets a
 //      zero / non-finite pivot or a pivot ratio below 1 / cond_limit (condition
-//      estimate), the refinement contracts by less than 2x per step or runs out
-//      of iterations, or the reference's own residual test (matrix_cpu.c:162-187)
+//      estimate), a refinement step contracts by less than cond_limit * 4 u32
+//      or it runs out of iterations, or the reference's own residual test (matrix_cpu.c:162-187)
 //      could land within a factor 256 n u of its 1e-6 threshold for this x, in
 //      which case only the exact FP64 solution can decide codes 2 / 3.
 // Everything that reaches the caller from the FP32 path therefore has status 0,
@@ -24,8 +24,8 @@ namespace ss {
 __host__ __device__ inline MixedParams default_mixed_params() {
   MixedParams p;
   p.max_iter = 12;
-  p.tol = 4.0e-16;
-  p.cond_limit = 1.0e7;
+  p.tol = 1.0e-14;
+  p.cond_limit = 1.0e3;
   p.resid_margin = 1.0e-8;
   return p;
 }
@@ -190,7 +190,8 @@ small_mixed_solve_kernel(BatchView bv, MixedParams mp) {
         }
         if (!(rel == rel) || !(dmax == dmax)) break;     // non-finite: let FP64 decide
         if (rel <= mp.tol) { conv = true; break; }
-        if (it > 0 && dmax > 0.5 * dprev) break;         // contraction too slow: stalled
+        // contraction slower than cond_limit * u32 allows: the estimate was optimistic
+        if (it > 0 && dmax > dprev * mp.cond_limit * 2.384185791015625e-07) break;
         dprev = dmax;
       }
       if (!conv) {

@@ -93,7 +93,7 @@ __device__ __forceinline__ bool small_exact_factor(SmallSmem<NP>& sm, double (&a
       if (ujj == 0.0) {
         sing = true;   // lu.c:540 singular(): the result is decided
       } else {
-        const double rinv = div_rn(1.0, ujj);
+        const double rinv = __drcp_rn(ujj);   // correctly rounded, = fl(1/ujj)
         if (KIND == kSolve) {
           if (act && !was_done && lane != p) {
             const double l = gsl_multiplier(a[j], ujj, rinv);
@@ -225,7 +225,7 @@ small_exact_kernel(BatchView bv) {
       const int code = small_exact_solve<NP, G>(sm, bv.b + ov, bv.out + ov, n, lane, gmask);
       if (lane == 0) {
         bv.status[s] = code;
-        if (bv.diag) bv.diag[s] = 0;
+        if (bv.diag) bv.diag[s] = kDiagExact;
       }
     } else {
       const bool act = lane < n;
@@ -261,7 +261,7 @@ small_exact_kernel(BatchView bv) {
       }
       if (lane == 0) {
         bv.status[s] = sing ? kInvertSingular : kOk;
-        if (bv.diag) bv.diag[s] = 0;
+        if (bv.diag) bv.diag[s] = kDiagExact;
       }
     }
     __syncwarp(gmask);

@@ -34,7 +34,8 @@ constexpr double kResidEps = 1.0e-6;
 constexpr double kDblMin = 2.2250738585072014e-308;
 
 // Per-system diagnostic bits written to the optional diag array.
-constexpr int kDiagFallback = 1 << 8;     // mixed path re-ran the system in exact FP64
+constexpr int kDiagExact = 1 << 8;        // result produced by the GSL-exact FP64 path
+constexpr int kDiagFallback = kDiagExact; // (mixed mode: the refinement did not accept it)
 constexpr int kDiagNoConverge = 1 << 9;   // refinement stalled (reason for fallback)
 constexpr int kDiagIllCond = 1 << 10;     // condition estimate above threshold
 constexpr int kDiagIterMask = 0xff;       // refinement iterations used

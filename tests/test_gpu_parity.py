@@ -139,24 +139,68 @@ def test_batched_device_plan_and_graph(engine):
 
 
 # ----------------------------------------------------------------- mixed ----
-def test_mixed_golden_codes_and_values(engine, golden_solve):
-    batch = batch_from_golden(golden_solve, "solve")
-    x, st = engine.solve_batched(batch, engine.MIXED)
-    np.testing.assert_array_equal(st, golden_solve["status_ref"])
-    ok = st == 0
-    m = np.repeat(ok, batch.n)
-    sub_off = np.zeros(int(ok.sum()), np.int64)
-    sub_n = batch.n[ok]
-    sub_off[1:] = np.cumsum(sub_n[:-1])
-    assert population_rel_err(x[m], golden_solve["x_ref"][m], sub_n, sub_off) <= POP_TOL
+def run_plan(engine, batch, mode):
+    import torch
+    dev = torch.device("cuda")
+    A = torch.from_numpy(batch.A).to(dev)
+    b = torch.from_numpy(batch.b).to(dev)
+    x = torch.full_like(b, float("nan"))
+    st = torch.full((batch.nsys,), -1, dtype=torch.int32, device=dev)
+    diag = torch.zeros((batch.nsys,), dtype=torch.int32, device=dev)
+    plan = engine.Plan(batch, mode)
+    plan.execute(A, x, st, b=b, diag=diag)
+    torch.cuda.synchronize()
+    plan.close()
+    return x.cpu().numpy(), st.cpu().numpy(), diag.cpu().numpy()
 
 
-def test_mixed_config0_accuracy(engine):
-    batch = wl.config0()
-    x, st = engine.solve_batched(batch, engine.MIXED)
+def check_mixed(engine, batch, require_accept=None):
+    """Codes exact; fallback systems bit-identical to the reference; accepted
+    systems within 1e-10 of the reference on significant populations, or, where
+    the reference's own FP64 answer is off by more, within 1e-10 of the exact
+    solution (80-digit mpmath)."""
+    x, st, diag = run_plan(engine, batch, engine.MIXED)
     xr, sr = oracle.solve(batch, "port", threads=oracle.host_threads())
     np.testing.assert_array_equal(st, sr)
-    assert population_rel_err(x, xr, batch.n, batch.offv) <= POP_TOL
-    for s in range(0, batch.nsys, 131):
+    fell_back = (diag & (1 << 8)) != 0
+    accepted = 0
+    for s in range(batch.nsys):
         n, o = int(batch.n[s]), int(batch.offv[s])
-        assert backward_err(batch.matrix(s), x[o:o + n], batch.rhs(s)) <= n * 1e-15
+        v, r = x[o:o + n], xr[o:o + n]
+        if fell_back[s]:
+            if st[s] != 4:
+                assert same_values(v, r).all(), s
+            continue
+        accepted += 1
+        assert st[s] == 0
+        if population_rel_err(v, r, np.array([n]), np.array([0])) > POP_TOL:
+            t = exact_solution(batch.matrix(s), batch.rhs(s))
+            assert population_rel_err(v, t, np.array([n]), np.array([0])) <= POP_TOL, s
+            assert population_rel_err(r, t, np.array([n]), np.array([0])) > POP_TOL, s
+    if require_accept is not None:
+        assert accepted >= require_accept * batch.nsys, (accepted, batch.nsys)
+    return accepted
+
+
+def exact_solution(A, b):
+    import mpmath
+    mpmath.mp.dps = 80
+    x = mpmath.lu_solve(mpmath.matrix(A.tolist()), mpmath.matrix(b.tolist()))
+    return np.array([float(t) for t in x])
+
+
+def test_mixed_golden(engine, golden_solve):
+    check_mixed(engine, batch_from_golden(golden_solve, "solve"))
+
+
+def test_mixed_config0(engine):
+    check_mixed(engine, wl.config0())
+
+
+def test_mixed_well_conditioned_sets_accept_and_match(engine):
+    rng = np.random.default_rng(77)
+    mats = [wl.macro_matrix(rng, int(n)) for n in rng.integers(4, 33, 600)]
+    macro = wl.from_matrices("solve", mats, [np.abs(rng.standard_normal(m.shape[0])) for m in mats])
+    check_mixed(engine, macro, require_accept=0.5)
+    dense = wl.dense_batch("solve", rng.integers(2, 33, 600), seed=78)
+    check_mixed(engine, dense, require_accept=0.3)
