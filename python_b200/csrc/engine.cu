@@ -103,17 +103,17 @@ static KernelSpec small_spec(int cls, int mode) {
 template <int KIND>
 static KernelSpec cta_spec(int cls) {
   KernelSpec k;
-#define SS_CTA(I, TR, TC, RB, CB)                                                       \
+#define SS_CTA(I, TG, B)                                                                \
   case I:                                                                               \
-    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, TR, TC, RB, CB>);      \
-    k.threads = TR * TC;                                                                \
-    k.dyn_smem = CtaShape<KIND, TR, TC, RB, CB>::dyn_smem;                              \
+    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, TG, B>);               \
+    k.threads = TG * TG;                                                                \
+    k.dyn_smem = CtaShape<KIND, TG, B>::dyn_smem;                                       \
     break;
   switch (cls) {
-    SS_CTA(0, 8, 8, 6, 6)
-    SS_CTA(1, 8, 8, 8, 8)
-    SS_CTA(2, 16, 8, 6, 12)
-    SS_CTA(3, 16, 16, 8, 8)
+    SS_CTA(0, 8, 6)
+    SS_CTA(1, 8, 8)
+    SS_CTA(2, 16, 6)
+    SS_CTA(3, 16, 8)
     default: break;
   }
 #undef SS_CTA
@@ -134,7 +134,7 @@ static int finish_spec(KernelSpec& k) {
     set_error("no kernel for this size class");
     return SIROCCO_ESIZE;
   }
-  if (k.dyn_smem > 48 * 1024)
+  if (k.dyn_smem > 0)
     SS_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k.dyn_smem)));
   int nb = 0;
   SS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.fn, k.threads, k.dyn_smem));

@@ -1,227 +1,290 @@
 // CTA-per-system kernels for 32 < n <= 128 (macro-atom jumping matrices of a
 // few dozen levels, per-element macro populations).
 //
-// The padded P x P matrix lives in registers: a TR x TC thread grid where the
-// thread (tr, tc) owns rows [tr*RB, tr*RB+RB) and columns [tc*CB, tc*CB+CB);
-// a warp covers 32/TC whole thread rows, so every thread finds the owner of
-// (its row, column j) in its own warp.  Rows never move; each row carries its
-// current position.  Step j:
-//   A  owners of column j propose their best (|a_rj|, pos) row, reduced across
-//      the owner lanes of each warp by shuffles, one candidate per warp to
-//      shared memory;                                          -- barrier
-//   B  every thread reduces the per-warp candidates (same answer everywhere),
-//      updates row positions, takes its rows' column-j entries from the owner
-//      lane by shuffle and forms its own multipliers; the pivot row's owners
-//      publish that row;                                      -- barrier
-//   C  every thread applies the rank-1 update to its RB x CB block.
-// Register indices stay compile-time constants: the element of column j in a
-// thread's block is picked with a short predicated chain.
-//
-// Arithmetic: as in kernels_small.cuh (GSL-exact below-pivot updates; the
-// solve's triangular sweeps follow LU_svx's order, run by one warp from a
-// shared-memory copy of the factors).
+// The padded P x P matrix lives in registers: a TG x TG thread grid, thread
+// (tr, tc) owning the B x B block of rows [tr*B, tr*B+B) and columns
+// [tc*B, tc*B+B).  The factorisation is blocked by panels of B columns, so the
+// panel of block column jb is exactly thread column jb and its pivot rows are
+// exactly thread row jb; every register index is a compile-time constant.
+// Per panel:
+//   1. the panel's owners copy it (all rows) to shared memory;
+//   2. warp 0 factorises the n x B panel there with physical row swaps, as
+//      GSL's LU_decomp_L2 does on a panel (lu.c:129-191): first strict maximum
+//      pivot, multipliers a * fl(1/u) (a / u below DBL_MIN), each update one
+//      rounding per product and per difference; every row's multipliers are
+//      recorded (M, n x B);
+//   3. the panel's row swaps are applied to the other columns (apply_pivots,
+//      lu.c:263) by moving the affected rows through shared memory;
+//   4. thread row jb rebuilds the pivot rows' values at their own step,
+//      V_k = W_k - sum_{k'<k} M[k][k'] V_k' (the dtrsm of lu.c:266);
+//   5. every other block takes W -= M V with k ascending (the dgemm of lu.c:269).
+// Every entry of the LU region therefore sees GSL's operation sequence.  For an
+// inverse the same sweep is an in-place Gauss-Jordan: rows above the panel and
+// columns left of it are eliminated too (fused multiply-add is allowed there,
+// outside the LU region), pivot rows are scaled by 1/u_kk, and the columns are
+// unscrambled in reverse pivot order at the end.  A solve keeps the LU factors
+// and runs LU_svx's triangular sweeps in GSL's order from shared memory.
 #pragma once
 #include "ss_common.cuh"
 
 namespace ss {
 
-// v[c] for a run-time c in [0, W) without dynamic register indexing
-template <int W>
-__device__ __forceinline__ double pick(const double (&v)[W], int c) {
-  double x = v[0];
-#pragma unroll
-  for (int i = 1; i < W; ++i) x = (c == i) ? v[i] : x;
-  return x;
-}
-
-template <int KIND, int TR, int TC, int RB, int CB>
+template <int KIND, int TG, int B>
 struct CtaShape {
-  static constexpr int P = TR * RB;
-  static constexpr int NT = TR * TC;
+  static constexpr int P = TG * B;         // padded order
+  static constexpr int NT = TG * TG;       // threads
   static constexpr int NW = NT / 32;
-  static constexpr int LS = P + 1;                          // LU row stride in shared memory
-  static constexpr size_t dyn_smem = (KIND == kSolve) ? size_t(P) * LS * sizeof(double) : 0;
-  // resident CTAs per SM asked of the register allocator: about 3 registers
-  // per owned element plus a fixed ~48 for indices and the step state
-  static constexpr int regs = 48 + 3 * RB * CB;
-  static constexpr int min_blocks = (65536 / (NT * (regs > 255 ? 255 : regs))) < 1 ? 1 : (65536 / (NT * (regs > 255 ? 255 : regs)));
-  static_assert(TC * CB == P, "square padding");
-  static_assert(TC <= 32 && (32 % TC) == 0, "column groups tile a warp");
+  static constexpr int PS = B + 1;         // panel row stride (odd)
+  static constexpr int LS = P + 1;         // LU row stride for the solve sweeps
+  // shared-memory layout (doubles): panel, multipliers, V, moved rows, scalars
+  static constexpr int off_M = P * PS;
+  static constexpr int off_V = 2 * P * PS;
+  static constexpr int off_R = off_V + B * P;
+  static constexpr int off_S = off_R + 2 * B * P;
+  static constexpr int n_dbl = off_S + 2 * B;
+  static constexpr int n_int = 4 * P + 8;  // ipiv, perm, slot_src, slot_dst, flags
+  static constexpr size_t panel_bytes = size_t(n_dbl) * 8 + size_t(n_int) * 4;
+  static constexpr size_t lu_bytes = size_t(P) * LS * 8 + size_t(2 * P) * 8 + size_t(P) * 4;
+  static constexpr size_t dyn_smem = (KIND == kSolve && lu_bytes > panel_bytes) ? lu_bytes : panel_bytes;
+  static constexpr int regs = 56 + 5 * B * B / 2;
+  static constexpr int min_blocks = (65536 / (NT * (regs > 255 ? 255 : regs))) < 1
+                                        ? 1 : (65536 / (NT * (regs > 255 ? 255 : regs)));
   static_assert(NT % 32 == 0, "whole warps");
+  static_assert(NT >= P, "one thread per row for the per-panel resets");
 };
 
-template <int KIND, int TR, int TC, int RB, int CB>
-__global__ void __launch_bounds__(TR * TC, (CtaShape<KIND, TR, TC, RB, CB>::min_blocks))
+template <int KIND, int TG, int B>
+__global__ void __launch_bounds__(TG * TG, (CtaShape<KIND, TG, B>::min_blocks))
 cta_exact_kernel(BatchView bv) {
-  using Sh = CtaShape<KIND, TR, TC, RB, CB>;
+  using Sh = CtaShape<KIND, TG, B>;
   constexpr int P = Sh::P;
-  constexpr int NW = Sh::NW;
-  constexpr int LS = Sh::LS;
-
-  __shared__ __align__(16) double ubuf[P];
-  __shared__ double ckey[NW], cval[NW];
-  __shared__ int cpk[NW];
-  __shared__ int ipiv[P];
-  __shared__ int cmap[P];
-  __shared__ int csrc[P];
-  __shared__ double vec[P];
-  __shared__ double xs[P];
-  extern __shared__ __align__(16) double lu_s[];
+  constexpr int PS = Sh::PS;
+  extern __shared__ __align__(16) double dsm[];
+  double* Pn = dsm;                      // [P][PS] panel
+  double* Mm = dsm + Sh::off_M;          // [P][PS] multipliers of this panel
+  double* Vs = dsm + Sh::off_V;          // [B][P]  pivot rows at their step
+  double* Rs = dsm + Sh::off_R;          // [2B][P] rows moved by the swaps
+  double* rinv_s = dsm + Sh::off_S;      // [B]
+  int* ipiv = reinterpret_cast<int*>(dsm + Sh::n_dbl);   // [P]
+  int* perm = ipiv + P;                  // [P] source row of each row after this panel's swaps
+  int* slot_src = perm + P;              // [P] staging slot of a row that moves, -1 otherwise
+  int* slot_dst = slot_src + P;          // [P] staging slot a row is refilled from, -1 otherwise
+  int* flags = slot_dst + P;             // [0] singular
 
   const int t = threadIdx.x;
-  const int tr = t / TC, tc = t % TC;
+  const int tr = t / TG, tc = t % TG;
+  const int row0 = tr * B, col0 = tc * B;
   const int wid = t >> 5, wl = t & 31;
-  const int row0 = tr * RB, col0 = tc * CB;
-  const int grp_lane0 = wl & ~(TC - 1);       // lane of (this thread row, tc = 0)
 
   for (int item = blockIdx.x; item < bv.count; item += gridDim.x) {
     const int s = bv.list[item];
     const int n = bv.n[s];
     const double* __restrict__ Ag = bv.A + bv.offA[s];
 
-    double a[RB][CB];
-    int pos[RB];
+    double a[B][B];
 #pragma unroll
-    for (int r = 0; r < RB; ++r) {
+    for (int r = 0; r < B; ++r) {
       const int row = row0 + r;
-      pos[r] = row;
 #pragma unroll
-      for (int c = 0; c < CB; ++c) {
+      for (int c = 0; c < B; ++c) {
         const int col = col0 + c;
-        a[r][c] = (row < n && col < n) ? Ag[int64_t(row) * n + col] : 0.0;
+        a[r][c] = (row < n && col < n) ? __ldg(Ag + int64_t(row) * n + col) : 0.0;
       }
     }
-    unsigned done = 0;
-    bool sing = false;
+    if (t == 0) flags[0] = 0;
 
-    for (int j = 0; j < n && !sing; ++j) {
-      const int jb = j / CB, cj = j - jb * CB;
-      // ---- A: candidates of column j --------------------------------------
-      double key = -1.0, val = 0.0;
-      int pk = 0x7fffffff;                     // (pos << 16) | row
+    const int npan = (n + B - 1) / B;
+    for (int jb = 0; jb < npan; ++jb) {
+      const int j0 = jb * B;
+      const int nb = min(B, n - j0);
+      // ---- 1. panel to shared memory, per-panel bookkeeping reset ----------
+      if (t < P) { slot_src[t] = -1; slot_dst[t] = -1; perm[t] = t; }
       if (tc == jb) {
 #pragma unroll
-        for (int r = 0; r < RB; ++r) {
-          const int row = row0 + r;
-          const double arj = pick<CB>(a[r], cj);
-          if (row < n && !((done >> r) & 1u)) {
-            const double k = pivot_key(arj);
-            const int pp = (pos[r] << 16) | row;
-            if (pivot_better(k, pp, key, pk)) { key = k; pk = pp; val = arj; }
-          }
-        }
-      }
+        for (int r = 0; r < B; ++r)
 #pragma unroll
-      for (int off = TC; off < 32; off <<= 1) {
-        const double ok = __shfl_xor_sync(0xffffffffu, key, off);
-        const double ov = __shfl_xor_sync(0xffffffffu, val, off);
-        const int op = __shfl_xor_sync(0xffffffffu, pk, off);
-        if (pivot_better(ok, op, key, pk)) { key = ok; pk = op; val = ov; }
-      }
-      if (wl == jb) { ckey[wid] = key; cval[wid] = val; cpk[wid] = pk; }
-      __syncthreads();
-
-      // ---- B: the pivot, positions, multipliers, published pivot row -------
-      key = -1.0; pk = 0x7fffffff; val = 0.0;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        const double k = ckey[w];
-        const int pp = cpk[w];
-        if (pivot_better(k, pp, key, pk)) { key = k; pk = pp; val = cval[w]; }
-      }
-      const int p = pk & 0xffff, ppos = pk >> 16;
-      const double ujj = val;
-      const unsigned was_done = done;
-#pragma unroll
-      for (int r = 0; r < RB; ++r) {
-        if (row0 + r == p) { pos[r] = j; done |= 1u << r; }
-        else if (pos[r] == j) pos[r] = ppos;
-      }
-      if (t == 0) ipiv[j] = ppos;
-      if (ujj == 0.0) {
-        sing = true;                           // uniform: every thread read the same ujj
-        continue;
-      }
-      const double rinv = __drcp_rn(ujj);      // correctly rounded, = fl(1/ujj)
-      const int prb = p / RB, prr = p - prb * RB;
-      // multipliers of this thread's rows; column j lives in lane (tr, jb)
-      double lr[RB];
-#pragma unroll
-      for (int r = 0; r < RB; ++r) {
-        const double mine = pick<CB>(a[r], cj);
-        const double arj = __shfl_sync(0xffffffffu, mine, grp_lane0 + jb);
-        const int row = row0 + r;
-        double l = 0.0;
-        if (row < n && row != p) {
-          if (!((was_done >> r) & 1u)) l = gsl_multiplier(arj, ujj, rinv);
-          else if (KIND == kInvert) l = mul_rn(arj, rinv);
-        }
-        lr[r] = l;
-      }
-      if (tr == prb) {
-#pragma unroll
-        for (int r = 0; r < RB; ++r)
-          if (r == prr) {
-#pragma unroll
-            for (int c = 0; c < CB; ++c) ubuf[col0 + c] = a[r][c];
+          for (int c = 0; c < B; ++c) {
+            Pn[(row0 + r) * PS + c] = a[r][c];
+            Mm[(row0 + r) * PS + c] = 0.0;
           }
       }
       __syncthreads();
 
-      // ---- C: rank-1 update ------------------------------------------------
-      double uc[CB];
+      // ---- 2. warp 0 factorises the panel --------------------------------
+      if (wid == 0) {
+        for (int k = 0; k < nb; ++k) {
+          const int j = j0 + k;
+          double bk = -1.0;
+          int br = 0x7fffffff;
+          for (int r = j + wl; r < n; r += 32) {
+            const double key = pivot_key(Pn[r * PS + k]);
+            if (pivot_better(key, r, bk, br)) { bk = key; br = r; }
+          }
 #pragma unroll
-      for (int c = 0; c < CB; ++c) uc[c] = ubuf[col0 + c];
-      const bool own_col = (tc == jb);
-      if (KIND == kInvert) {
-        // rows whose multiplier is 0 (the pivot row, padding) keep their values
+          for (int off = 16; off > 0; off >>= 1) {
+            const double ok = __shfl_xor_sync(0xffffffffu, bk, off);
+            const int orr = __shfl_xor_sync(0xffffffffu, br, off);
+            if (pivot_better(ok, orr, bk, br)) { bk = ok; br = orr; }
+          }
+          const int p = br;
+          if (wl == 0) ipiv[j] = p;
+          if (p != j && wl < B) {
+            const double x = Pn[j * PS + wl]; Pn[j * PS + wl] = Pn[p * PS + wl]; Pn[p * PS + wl] = x;
+            const double y = Mm[j * PS + wl]; Mm[j * PS + wl] = Mm[p * PS + wl]; Mm[p * PS + wl] = y;
+          }
+          __syncwarp();
+          const double ujj = Pn[j * PS + k];
+          if (ujj == 0.0) {
+            if (wl == 0) flags[0] = 1;
+            break;
+          }
+          const double rinv = __drcp_rn(ujj);   // correctly rounded, = fl(1/ujj)
+          double piv[B];
 #pragma unroll
-        for (int r = 0; r < RB; ++r) {
+          for (int c = 0; c < B; ++c) piv[c] = Pn[j * PS + c];
+          __syncwarp();
+          for (int r = wl; r < n; r += 32) {
+            if (r == j) continue;
+            if (KIND == kSolve && r < j) continue;
+            const double v = Pn[r * PS + k];
+            const double l = (r > j) ? gsl_multiplier(v, ujj, rinv) : mul_rn(v, rinv);
+            Mm[r * PS + k] = l;
 #pragma unroll
-          for (int c = 0; c < CB; ++c) a[r][c] = sub_rn(a[r][c], mul_rn(lr[r], uc[c]));
-        }
-        if (tr == prb) {
-#pragma unroll
-          for (int r = 0; r < RB; ++r)
-            if (r == prr) {
-#pragma unroll
-              for (int c = 0; c < CB; ++c) a[r][c] = mul_rn(a[r][c], rinv);
+            for (int c = 0; c < B; ++c) {
+              if (c == k || c >= nb) continue;
+              if (KIND == kSolve && c < k) continue;
+              Pn[r * PS + c] = sub_rn(Pn[r * PS + c], mul_rn(l, piv[c]));
             }
+            Pn[r * PS + k] = (KIND == kInvert) ? -l : l;
+          }
+          if (wl == 0) {
+            rinv_s[k] = rinv;
+            if (KIND == kInvert) {
+#pragma unroll
+              for (int c = 0; c < B; ++c) Pn[j * PS + c] = (c == k) ? rinv : mul_rn(piv[c], rinv);
+            }
+          }
+          __syncwarp();
         }
-        if (own_col) {
-          // column j becomes column j of the inverse-in-place: -l, and 1/u_jj on the pivot row
+        if (wl == 0 && flags[0] == 0) {
+          // net row permutation of this panel and the staging slots of moved rows
+          for (int k = 0; k < nb; ++k) {
+            const int q = ipiv[j0 + k];
+            if (q != j0 + k) { const int x = perm[j0 + k]; perm[j0 + k] = perm[q]; perm[q] = x; }
+          }
+          int m = 0;
+          for (int k = 0; k < nb; ++k) {
+            const int q = ipiv[j0 + k];
+            if (q == j0 + k) continue;
+            const int cand[2] = {j0 + k, q};
+            for (int ci = 0; ci < 2; ++ci) {
+              const int rr = cand[ci];
+              if (perm[rr] != rr && slot_dst[rr] < 0) {
+                slot_dst[rr] = m;
+                slot_src[perm[rr]] = m;
+                ++m;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (flags[0]) break;
+
+      // ---- 3. the panel's row swaps on the other columns ------------------
+      if (tc != jb) {
 #pragma unroll
-          for (int r = 0; r < RB; ++r) {
-            const double v = (row0 + r == p) ? rinv : -lr[r];
+        for (int r = 0; r < B; ++r) {
+          const int sl = slot_src[row0 + r];
+          if (sl >= 0) {
 #pragma unroll
-            for (int c = 0; c < CB; ++c)
-              if (c == cj) a[r][c] = v;
+            for (int c = 0; c < B; ++c) Rs[sl * P + col0 + c] = a[r][c];
+          }
+        }
+      }
+      __syncthreads();
+      if (tc != jb) {
+#pragma unroll
+        for (int r = 0; r < B; ++r) {
+          const int sl = slot_dst[row0 + r];
+          if (sl >= 0) {
+#pragma unroll
+            for (int c = 0; c < B; ++c) a[r][c] = Rs[sl * P + col0 + c];
+          }
+        }
+        // ---- 4. pivot rows at their own step (thread row jb) --------------
+        if (tr == jb && (KIND == kInvert || tc > jb)) {
+#pragma unroll
+          for (int k = 0; k < B; ++k) {
+            if (k < nb) {
+#pragma unroll
+              for (int c = 0; c < B; ++c) {
+                double v = a[k][c];
+#pragma unroll
+                for (int kk = 0; kk < k; ++kk)
+                  v = sub_rn(v, mul_rn(Mm[(j0 + k) * PS + kk], Vs[kk * P + col0 + c]));
+                Vs[k * P + col0 + c] = v;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+
+      // ---- 5. rank-nb update of this thread's block ------------------------
+      if (tc == jb) {
+#pragma unroll
+        for (int r = 0; r < B; ++r)
+#pragma unroll
+          for (int c = 0; c < B; ++c) a[r][c] = Pn[(row0 + r) * PS + c];
+      } else if (tr == jb) {
+        // the panel's pivot rows: their final values from V
+        if (KIND == kInvert || tc > jb) {
+#pragma unroll
+          for (int k = 0; k < B; ++k) {
+            if (k < nb) {
+#pragma unroll
+              for (int c = 0; c < B; ++c) {
+                double acc = Vs[k * P + col0 + c];
+                if (KIND == kInvert) {
+                  acc = acc * rinv_s[k];
+#pragma unroll
+                  for (int k2 = k + 1; k2 < B; ++k2)
+                    if (k2 < nb) acc = fma(-Mm[(j0 + k) * PS + k2], Vs[k2 * P + col0 + c], acc);
+                }
+                a[k][c] = acc;
+              }
+            }
           }
         }
       } else {
-        if (tc >= jb) {
+        const bool lu_region = (tr > jb) && (tc > jb);   // below the panel, right of it
+        if (KIND == kInvert || lu_region) {
 #pragma unroll
-          for (int r = 0; r < RB; ++r) {
+          for (int k = 0; k < B; ++k) {
+            if (k < nb) {
+              double vk[B];
 #pragma unroll
-            for (int c = 0; c < CB; ++c)
-              if (tc > jb || c > cj) a[r][c] = sub_rn(a[r][c], mul_rn(lr[r], uc[c]));
-          }
-        }
-        if (own_col) {
+              for (int c = 0; c < B; ++c) vk[c] = Vs[k * P + col0 + c];
 #pragma unroll
-          for (int r = 0; r < RB; ++r) {
-            const int row = row0 + r;
-            if (row < n && row != p && !((was_done >> r) & 1u)) {
+              for (int r = 0; r < B; ++r) {
+                const double m = Mm[(row0 + r) * PS + k];
+                if (lu_region) {
 #pragma unroll
-              for (int c = 0; c < CB; ++c)
-                if (c == cj) a[r][c] = lr[r];
+                  for (int c = 0; c < B; ++c) a[r][c] = sub_rn(a[r][c], mul_rn(m, vk[c]));
+                } else {
+#pragma unroll
+                  for (int c = 0; c < B; ++c) a[r][c] = fma(-m, vk[c], a[r][c]);
+                }
+              }
             }
           }
         }
       }
+      __syncthreads();
     }
 
-    if (sing) {
+    if (flags[0]) {
       if (t == 0) {
         bv.status[s] = (KIND == kSolve) ? kSolveSingular : kInvertSingular;
         if (bv.diag) bv.diag[s] = kDiagExact;
@@ -231,26 +294,26 @@ cta_exact_kernel(BatchView bv) {
     }
 
     if (KIND == kInvert) {
-      // reverse-order column unscramble: output column cmap[k] takes column k
+      // reverse-order column unscramble: output column perm[k] takes column k
       if (t == 0) {
-        for (int c = 0; c < n; ++c) csrc[c] = c;
+        int* src = slot_src;
+        for (int c = 0; c < n; ++c) src[c] = c;
         for (int jj = n - 1; jj >= 0; --jj) {
           const int q = ipiv[jj];
-          if (q != jj) { const int tmp = csrc[jj]; csrc[jj] = csrc[q]; csrc[q] = tmp; }
+          if (q != jj) { const int x = src[jj]; src[jj] = src[q]; src[q] = x; }
         }
-        for (int c = 0; c < n; ++c) cmap[csrc[c]] = c;
+        for (int c = 0; c < n; ++c) perm[src[c]] = c;
       }
       __syncthreads();
       double* __restrict__ Og = bv.out + bv.offA[s];
 #pragma unroll
-      for (int r = 0; r < RB; ++r) {
+      for (int r = 0; r < B; ++r) {
         const int row = row0 + r;
         if (row < n) {
-          const int64_t ro = int64_t(pos[r]) * n;
 #pragma unroll
-          for (int c = 0; c < CB; ++c) {
+          for (int c = 0; c < B; ++c) {
             const int col = col0 + c;
-            if (col < n) Og[ro + cmap[col]] = a[r][c];
+            if (col < n) Og[int64_t(row) * n + perm[col]] = a[r][c];
           }
         }
       }
@@ -259,33 +322,49 @@ cta_exact_kernel(BatchView bv) {
         if (bv.diag) bv.diag[s] = kDiagExact;
       }
     } else {
-      // factors into shared memory by position; cmap[i] = original row at position i
+      // LU (rows already in GSL's order) into shared memory for the sweeps;
+      // the pivots survive in ipiv, which the LU copy does not overlap
+      constexpr int LS = Sh::LS;
+      double* lu = dsm;
+      double* vec = dsm + P * LS;
+      double* xs = vec + P;
+      int* pm = reinterpret_cast<int*>(xs + P);
+      // the pivots sit inside the area the LU copy overwrites: move them first
+      if (t < n) pm[t] = ipiv[t];
+      __syncthreads();
 #pragma unroll
-      for (int r = 0; r < RB; ++r) {
-        const int row = row0 + r;
-        if (row < n) {
+      for (int r = 0; r < B; ++r)
 #pragma unroll
-          for (int c = 0; c < CB; ++c) lu_s[pos[r] * LS + col0 + c] = a[r][c];
-          if (tc == 0) cmap[pos[r]] = row;
-        }
-      }
+        for (int c = 0; c < B; ++c) lu[(row0 + r) * LS + col0 + c] = a[r][c];
       __syncthreads();
       if (wid == 0) {
         const int64_t ov = bv.offv[s];
-        for (int i = wl; i < n; i += 32) vec[i] = bv.b[ov + cmap[i]];
+        // gsl_permutation from the row swaps (lu.c:95-109), built in place of
+        // the pivots: pm[i] = original row now at i
+        if (wl == 0) {
+          int* sw = reinterpret_cast<int*>(vec);   // scratch copy of the pivots
+          for (int i = 0; i < n; ++i) sw[i] = pm[i];
+          for (int i = 0; i < n; ++i) pm[i] = i;
+          for (int i = 0; i < n; ++i) {
+            const int q = sw[i];
+            if (pm[q] != pm[i]) { const int x = pm[q]; pm[q] = pm[i]; pm[i] = x; }
+          }
+        }
+        __syncwarp();
+        for (int i = wl; i < n; i += 32) vec[i] = bv.b[ov + pm[i]];
         __syncwarp();
         // forward sweep (unit L), ascending j per entry
         for (int j = 0; j < n; ++j) {
           const double yj = vec[j];
-          for (int i = j + 1 + wl; i < n; i += 32) vec[i] = sub_rn(vec[i], mul_rn(lu_s[i * LS + j], yj));
+          for (int i = j + 1 + wl; i < n; i += 32) vec[i] = sub_rn(vec[i], mul_rn(lu[i * LS + j], yj));
           __syncwarp();
         }
         // backward sweep in LU_svx's order (serial chain)
         if (wl == 0) {
           for (int i = n - 1; i >= 0; --i) {
             double u = vec[i];
-            for (int k = i + 1; k < n; ++k) u = sub_rn(u, mul_rn(lu_s[i * LS + k], xs[k]));
-            xs[i] = div_rn(u, lu_s[i * LS + i]);
+            for (int k = i + 1; k < n; ++k) u = sub_rn(u, mul_rn(lu[i * LS + k], xs[k]));
+            xs[i] = div_rn(u, lu[i * LS + i]);
           }
         }
         __syncwarp();

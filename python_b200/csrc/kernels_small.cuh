@@ -42,14 +42,29 @@ __device__ __forceinline__ unsigned group_mask() {
   return (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wlane & ~(G - 1)));
 }
 
-// Coalesced load of system s into sm.stage.
+// Coalesced load of system s into sm.stage, every load of the lane issued
+// before the first shared-memory store so they are all in flight together.
 template <int NP, int G>
 __device__ __forceinline__ void small_stage(SmallSmem<NP>& sm, const double* __restrict__ Ag, int n, int lane,
                                             unsigned gmask) {
   constexpr int S = SmallSmem<NP>::S;
-  for (int e = lane; e < n * n; e += G) {
-    const int r = e / n;
-    sm.stage[r * S + (e - r * n)] = Ag[e];
+  constexpr int PER = (NP * NP + G - 1) / G;
+  const int nn = n * n;
+  double v[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = lane + u * G;
+    v[u] = (e < nn) ? __ldg(Ag + e) : 0.0;
+  }
+  // element e = r * n + c; track (r, c) incrementally instead of dividing
+  int r = lane / n, c = lane - (lane / n) * n;
+  const int dr = G / n, dc = G - (G / n) * n;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    if (lane + u * G < nn) sm.stage[r * S + c] = v[u];
+    r += dr;
+    c += dc;
+    if (c >= n) { c -= n; ++r; }
   }
   __syncwarp(gmask);
 }
