@@ -110,6 +110,26 @@ int sirocco_plan_destroy(sirocco_plan *plan);
 /* Text of the last library error on this thread. */
 const char *sirocco_last_error(void);
 
+/* No counterpart in the reference.  Batched solve that allocates no memory at
+   all, for callers that cannot let a library allocate on the GPU: host codes
+   that reserve the device's memory up front for their own arena (a cudaMalloc
+   from a library then fails, or eats the budget of the other MPI ranks sharing
+   the GPU), and codes that must not pay the device-wide synchronisation that
+   cudaMalloc / cudaFree bring while other streams are busy.  Everything is a
+   device pointer, the layout arrays n / offA / offv included; nmax is the
+   largest order in the batch, at most SIROCCO_NOALLOC_MAX_N (larger returns
+   SIROCCO_ESIZE; a system above nmax gets status -1).  Results and codes are
+   those of solve_matrix_batched (GSL-exact FP64).  The factorisation scratch is
+   a static device array of SIROCCO_NOALLOC_SLABS x MAX_N^2 doubles (16 MiB)
+   that every GPU loading this library holds until exit; its address is looked
+   up on the first call on each device.  All calls share that array, so calls
+   whose work overlaps on the GPU (other streams, other host threads) race:
+   serialise them.  The call only enqueues work on `stream`. */
+#define SIROCCO_NOALLOC_MAX_N 512
+#define SIROCCO_NOALLOC_SLABS 8
+int solve_matrix_batched_noalloc(int nsys, int nmax, const int *n, const int64_t *offA, const double *A,
+                                 const int64_t *offv, const double *b, double *x, int *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -625,6 +626,48 @@ static int run_single(int kind, double* A, const double* b, int size, double* ou
 
 }  // namespace ss
 
+namespace ss {
+
+// ---------------------------------------------------------- no-allocation --
+// Scratch of solve_matrix_batched_noalloc: one n x n slab per resident CTA of the
+// n > 128 solve kernel, in a file-scope device array instead of cudaMalloc'd
+// memory.  Every GPU that loads this library holds the array until the process
+// exits; every call shares it and overwrites what the previous call left there.
+constexpr int kNoAllocMaxN = SIROCCO_NOALLOC_MAX_N;
+constexpr int kNoAllocSlabs = SIROCCO_NOALLOC_SLABS;
+constexpr int64_t kNoAllocSlab = int64_t(kNoAllocMaxN) * kNoAllocMaxN;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlabs * kNoAllocSlab];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kMaxDevices] = {};
+
+// The array's device address on the current device.  In host code the symbol
+// g_noalloc_scratch is only a host-side handle, so the address is looked up once
+// per device with that device current, then reused.
+static int noalloc_scratch(double** out) {
+  int dev = 0;
+  SS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device %d beyond the %d devices the no-allocation path tracks", dev, kMaxDevices);
+    return SIROCCO_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      set_error("cudaGetSymbolAddress of the no-allocation scratch failed: %s", cudaGetErrorString(e));
+      return int(e);
+    }
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+}  // namespace ss
+
 // ===================================================================== C ABI ==
 using namespace ss;
 
@@ -734,5 +777,42 @@ int sirocco_plan_destroy(sirocco_plan* plan) {
 }
 
 const char* sirocco_last_error(void) { return g_last_error.c_str(); }
+
+int solve_matrix_batched_noalloc(int nsys, int nmax, const int* n, const int64_t* offA, const double* A,
+                                 const int64_t* offv, const double* b, double* x, int* status, void* stream) {
+  if (nsys == 0) return 0;
+  if (nsys < 0 || !n || !offA || !A || !offv || !b || !x || !status) {
+    set_error("invalid arguments to solve_matrix_batched_noalloc");
+    return SIROCCO_EINVAL;
+  }
+  if (nmax < 1 || nmax > kNoAllocMaxN) {
+    set_error("solve_matrix_batched_noalloc: largest order %d outside 1..%d, the size of its static scratch",
+              nmax, kNoAllocMaxN);
+    return SIROCCO_ESIZE;
+  }
+  double* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  const void* fn = reinterpret_cast<const void*>(&global_exact_kernel<kSolve, true>);
+  const size_t smem = global_smem_bytes(nmax);
+  SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  BatchView v;
+  v.n = n;
+  v.offA = offA;
+  v.offv = offv;
+  v.A = A;
+  v.b = b;
+  v.out = x;
+  v.status = status;
+  v.diag = nullptr;
+  v.list = nullptr;
+  v.count = nsys;
+  int64_t slab = int64_t(nmax) * nmax;
+  // every CTA works in its own slab: no more CTAs than slabs of this size fit
+  const int grid = int(std::min<int64_t>(std::min<int64_t>(nsys, 1024), int64_t(kNoAllocSlabs) * kNoAllocSlab / slab));
+  void* args[] = {&v, &nmax, &scratch, &slab};
+  SS_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(kGThreads), args, smem, static_cast<cudaStream_t>(stream)));
+  return 0;
+}
 
 }  // extern "C"

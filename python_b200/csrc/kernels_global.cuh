@@ -33,7 +33,10 @@ __host__ __device__ constexpr size_t global_smem_bytes(int nmax) {
        + size_t(32) * sizeof(double);                  // per-step scalars
 }
 
-template <int KIND>
+// DIRECT = true is the variant behind solve_matrix_batched_noalloc: system
+// `item` is batch entry `item` (no bucket list) and a system larger than nmax
+// is refused with status -1 instead of being factorised.
+template <int KIND, bool DIRECT = false>
 __global__ void __launch_bounds__(kGThreads, 1)
 global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
   extern __shared__ __align__(16) double gsm[];
@@ -51,8 +54,12 @@ global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
   const int wid = t >> 5, wl = t & 31;
 
   for (int item = blockIdx.x; item < bv.count; item += gridDim.x) {
-    const int s = bv.list[item];
+    const int s = DIRECT ? item : bv.list[item];
     const int n = bv.n[s];
+    if (DIRECT && (n < 1 || n > nmax)) {
+      if (t == 0) bv.status[s] = -1;
+      continue;
+    }
     const double* __restrict__ Ag = bv.A + bv.offA[s];
     double* __restrict__ W = (KIND == kInvert) ? bv.out + bv.offA[s] : scratch + int64_t(blockIdx.x) * slab;
     const int64_t nn = int64_t(n) * n;

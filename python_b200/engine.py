@@ -28,7 +28,7 @@ EXPORTS = (
     "gpu_solve_matrix", "gpu_invert_matrix",
     "solve_matrix_batched", "invert_matrix_batched", "sirocco_set_precision",
     "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
-    "sirocco_plan_destroy", "sirocco_last_error",
+    "sirocco_plan_destroy", "sirocco_last_error", "solve_matrix_batched_noalloc",
 )
 
 _lib = None
@@ -75,6 +75,8 @@ def load() -> ctypes.CDLL:
     lib.sirocco_plan_destroy.argtypes = [c_void_p]
     lib.sirocco_plan_destroy.restype = c_int
     lib.sirocco_last_error.restype = c_char_p
+    lib.solve_matrix_batched_noalloc.argtypes = [c_int, c_int] + [c_void_p] * 8
+    lib.solve_matrix_batched_noalloc.restype = c_int
     _lib = lib
     return lib
 
