@@ -41,12 +41,18 @@ struct CtaShape {
   static constexpr int off_V = 2 * P * PS;
   static constexpr int off_R = off_V + B * P;
   static constexpr int off_S = off_R + 2 * B * P;
-  static constexpr int n_dbl = off_S + 2 * B;
-  static constexpr int n_int = 4 * P + 8;  // ipiv, perm, slot_src, slot_dst, flags
+  static constexpr int n_dbl0 = off_S + 2 * B;
+  static constexpr int n_dbl = n_dbl0 > P * LS ? n_dbl0 : P * LS;
+  static constexpr int n_int = 5 * P + 8;  // ipiv, perm, slot_src, slot_dst, total, flags
+  static constexpr int PER = (P * P + NT - 1) / NT;   // staged elements per thread
   static constexpr size_t panel_bytes = size_t(n_dbl) * 8 + size_t(n_int) * 4;
   static constexpr size_t lu_bytes = size_t(P) * LS * 8 + size_t(2 * P) * 8 + size_t(P) * 4;
-  static constexpr size_t dyn_smem = (KIND == kSolve && lu_bytes > panel_bytes) ? lu_bytes : panel_bytes;
-  static constexpr int regs = 56 + 5 * B * B / 2;
+  // the whole matrix passes through shared memory (row stride LS) on its way
+  // in and out, so the global loads and stores are row-coalesced
+  static constexpr size_t stage_bytes = size_t(P) * LS * 8;
+  static constexpr size_t dyn_smem_a = (KIND == kSolve && lu_bytes > panel_bytes) ? lu_bytes : panel_bytes;
+  static constexpr size_t dyn_smem = dyn_smem_a > stage_bytes + size_t(n_int) * 4 + 64 ? dyn_smem_a : stage_bytes + size_t(n_int) * 4 + 64;
+  static constexpr int regs = 72 + 5 * B * B / 2;
   static constexpr int min_blocks = (65536 / (NT * (regs > 255 ? 255 : regs))) < 1
                                         ? 1 : (65536 / (NT * (regs > 255 ? 255 : regs)));
   static_assert(NT % 32 == 0, "whole warps");
@@ -69,7 +75,8 @@ cta_exact_kernel(BatchView bv) {
   int* perm = ipiv + P;                  // [P] source row of each row after this panel's swaps
   int* slot_src = perm + P;              // [P] staging slot of a row that moves, -1 otherwise
   int* slot_dst = slot_src + P;          // [P] staging slot a row is refilled from, -1 otherwise
-  int* flags = slot_dst + P;             // [0] singular
+  int* total = slot_dst + P;             // [P] original row now at each row (GSL's permutation)
+  int* flags = total + P;                // [0] singular
 
   const int t = threadIdx.x;
   const int tr = t / TG, tc = t % TG;
@@ -81,16 +88,30 @@ cta_exact_kernel(BatchView bv) {
     const int n = bv.n[s];
     const double* __restrict__ Ag = bv.A + bv.offA[s];
 
+    // coalesced load of the padded P x P matrix, every load of a thread in
+    // flight at once, through shared memory to the register blocks
+    {
+      double* stage = dsm;
+      double v[Sh::PER];
+#pragma unroll
+      for (int u = 0; u < Sh::PER; ++u) {
+        const int e = t + u * Sh::NT, row = e / P, col = e - (e / P) * P;
+        v[u] = (e < P * P && row < n && col < n) ? __ldg(Ag + int64_t(row) * n + col) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < Sh::PER; ++u) {
+        const int e = t + u * Sh::NT, row = e / P, col = e - (e / P) * P;
+        if (e < P * P) stage[row * Sh::LS + col] = v[u];
+      }
+      if (t < P) total[t] = t;
+      __syncthreads();
+    }
     double a[B][B];
 #pragma unroll
-    for (int r = 0; r < B; ++r) {
-      const int row = row0 + r;
+    for (int r = 0; r < B; ++r)
 #pragma unroll
-      for (int c = 0; c < B; ++c) {
-        const int col = col0 + c;
-        a[r][c] = (row < n && col < n) ? __ldg(Ag + int64_t(row) * n + col) : 0.0;
-      }
-    }
+      for (int c = 0; c < B; ++c) a[r][c] = dsm[(row0 + r) * Sh::LS + col0 + c];
+    __syncthreads();
     if (t == 0) flags[0] = 0;
 
     const int npan = (n + B - 1) / B;
@@ -99,6 +120,7 @@ cta_exact_kernel(BatchView bv) {
       const int nb = min(B, n - j0);
       // ---- 1. panel to shared memory, per-panel bookkeeping reset ----------
       if (t < P) { slot_src[t] = -1; slot_dst[t] = -1; perm[t] = t; }
+      if (t < B) rinv_s[t] = 0.0;     // padding steps of the last panel contribute nothing
       if (tc == jb) {
 #pragma unroll
         for (int r = 0; r < B; ++r)
@@ -110,81 +132,117 @@ cta_exact_kernel(BatchView bv) {
       }
       __syncthreads();
 
-      // ---- 2. warp 0 factorises the panel --------------------------------
+      // ---- 2. warp 0 factorises the panel in its registers -----------------
+      // Lane l holds panel rows l, l+32, ... (indexed by the row they had when
+      // the panel started); rows keep their place and carry their current
+      // position, so ties break as GSL's physical swaps would.  Multipliers and
+      // the factorised panel are stored by that origin row; perm[q] = origin of
+      // the row that ends at position q.
       if (wid == 0) {
-        for (int k = 0; k < nb; ++k) {
-          const int j = j0 + k;
-          double bk = -1.0;
-          int br = 0x7fffffff;
-          for (int r = j + wl; r < n; r += 32) {
-            const double key = pivot_key(Pn[r * PS + k]);
-            if (pivot_better(key, r, bk, br)) { bk = key; br = r; }
-          }
+        constexpr int RPL = (P + 31) / 32;
+        double pr[RPL][B];
+        int ps[RPL];
 #pragma unroll
-          for (int off = 16; off > 0; off >>= 1) {
-            const double ok = __shfl_xor_sync(0xffffffffu, bk, off);
-            const int orr = __shfl_xor_sync(0xffffffffu, br, off);
-            if (pivot_better(ok, orr, bk, br)) { bk = ok; br = orr; }
-          }
-          const int p = br;
-          if (wl == 0) ipiv[j] = p;
-          if (p != j && wl < B) {
-            const double x = Pn[j * PS + wl]; Pn[j * PS + wl] = Pn[p * PS + wl]; Pn[p * PS + wl] = x;
-            const double y = Mm[j * PS + wl]; Mm[j * PS + wl] = Mm[p * PS + wl]; Mm[p * PS + wl] = y;
-          }
-          __syncwarp();
-          const double ujj = Pn[j * PS + k];
-          if (ujj == 0.0) {
-            if (wl == 0) flags[0] = 1;
-            break;
-          }
-          const double rinv = __drcp_rn(ujj);   // correctly rounded, = fl(1/ujj)
-          double piv[B];
+        for (int i = 0; i < RPL; ++i) {
+          const int r = wl + 32 * i;
+          ps[i] = r;
 #pragma unroll
-          for (int c = 0; c < B; ++c) piv[c] = Pn[j * PS + c];
-          __syncwarp();
-          for (int r = wl; r < n; r += 32) {
-            if (r == j) continue;
-            if (KIND == kSolve && r < j) continue;
-            const double v = Pn[r * PS + k];
-            const double l = (r > j) ? gsl_multiplier(v, ujj, rinv) : mul_rn(v, rinv);
-            Mm[r * PS + k] = l;
-#pragma unroll
-            for (int c = 0; c < B; ++c) {
-              if (c == k || c >= nb) continue;
-              if (KIND == kSolve && c < k) continue;
-              Pn[r * PS + c] = sub_rn(Pn[r * PS + c], mul_rn(l, piv[c]));
-            }
-            Pn[r * PS + k] = (KIND == kInvert) ? -l : l;
-          }
-          if (wl == 0) {
-            rinv_s[k] = rinv;
-            if (KIND == kInvert) {
-#pragma unroll
-              for (int c = 0; c < B; ++c) Pn[j * PS + c] = (c == k) ? rinv : mul_rn(piv[c], rinv);
-            }
-          }
-          __syncwarp();
+          for (int c = 0; c < B; ++c) pr[i][c] = (r < n) ? Pn[r * PS + c] : 0.0;
         }
-        if (wl == 0 && flags[0] == 0) {
-          // net row permutation of this panel and the staging slots of moved rows
-          for (int k = 0; k < nb; ++k) {
-            const int q = ipiv[j0 + k];
-            if (q != j0 + k) { const int x = perm[j0 + k]; perm[j0 + k] = perm[q]; perm[q] = x; }
-          }
-          int m = 0;
-          for (int k = 0; k < nb; ++k) {
-            const int q = ipiv[j0 + k];
-            if (q == j0 + k) continue;
-            const int cand[2] = {j0 + k, q};
-            for (int ci = 0; ci < 2; ++ci) {
-              const int rr = cand[ci];
-              if (perm[rr] != rr && slot_dst[rr] < 0) {
-                slot_dst[rr] = m;
-                slot_src[perm[rr]] = m;
-                ++m;
+        bool sing = false;
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+          if (k < nb && !sing) {
+            const int j = j0 + k;
+            double bk = -1.0;
+            int bp = 0x7fffffff, bw = 0;
+#pragma unroll
+            for (int i = 0; i < RPL; ++i) {
+              const int r = wl + 32 * i;
+              if (r < n && ps[i] >= j) {
+                const double key = pivot_key(pr[i][k]);
+                if (pivot_better(key, ps[i], bk, bp)) { bk = key; bp = ps[i]; bw = (wl << 3) | i; }
               }
             }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+              const double ok = __shfl_xor_sync(0xffffffffu, bk, off);
+              const int op = __shfl_xor_sync(0xffffffffu, bp, off);
+              const int ow = __shfl_xor_sync(0xffffffffu, bw, off);
+              if (pivot_better(ok, op, bk, bp)) { bk = ok; bp = op; bw = ow; }
+            }
+            const int pl = bw >> 3, pi = bw & 7, ppos = bp;
+            if (wl == 0) ipiv[j] = ppos;
+#pragma unroll
+            for (int i = 0; i < RPL; ++i) {
+              if (wl == pl && i == pi) ps[i] = j;
+              else if (ps[i] == j) ps[i] = ppos;
+            }
+            double pv[B];
+#pragma unroll
+            for (int c = 0; c < B; ++c) {
+              double mine = pr[0][c];
+#pragma unroll
+              for (int i = 1; i < RPL; ++i) mine = (pi == i) ? pr[i][c] : mine;
+              pv[c] = __shfl_sync(0xffffffffu, mine, pl);
+            }
+            const double ujj = pv[k];
+            if (ujj == 0.0) {
+              sing = true;
+            } else {
+              const double rinv = __drcp_rn(ujj);   // correctly rounded, = fl(1/ujj)
+#pragma unroll
+              for (int i = 0; i < RPL; ++i) {
+                const int r = wl + 32 * i;
+                const bool is_piv = (wl == pl) && (i == pi);
+                if (r < n && !is_piv) {
+                  const bool below = ps[i] > j;
+                  if (KIND == kInvert || below) {
+                    const double l = below ? gsl_multiplier(pr[i][k], ujj, rinv) : mul_rn(pr[i][k], rinv);
+                    Mm[r * PS + k] = l;
+#pragma unroll
+                    for (int c = 0; c < B; ++c) {
+                      if (c == k || (KIND == kSolve && c < k)) continue;
+                      pr[i][c] = sub_rn(pr[i][c], mul_rn(l, pv[c]));
+                    }
+                    pr[i][k] = (KIND == kInvert) ? -l : l;
+                  }
+                }
+                if (KIND == kInvert && is_piv) {
+#pragma unroll
+                  for (int c = 0; c < B; ++c) pr[i][c] = (c == k) ? rinv : mul_rn(pr[i][c], rinv);
+                }
+              }
+              if (wl == 0) rinv_s[k] = rinv;
+            }
+          }
+        }
+        if (sing) {
+          if (wl == 0) flags[0] = 1;
+        } else {
+#pragma unroll
+          for (int i = 0; i < RPL; ++i) {
+            const int r = wl + 32 * i;
+            if (r < n) {
+#pragma unroll
+              for (int c = 0; c < B; ++c) Pn[r * PS + c] = pr[i][c];
+              perm[ps[i]] = r;
+            }
+          }
+          __syncwarp();
+          // staging slots of the rows whose content changes
+          int base = 0;
+#pragma unroll
+          for (int i = 0; i < RPL; ++i) {
+            const int q = wl + 32 * i;
+            const bool moved = (q < n) && (perm[q] != q);
+            const unsigned mask = __ballot_sync(0xffffffffu, moved);
+            if (moved) {
+              const int sl = base + __popc(mask & ((1u << wl) - 1u));
+              slot_dst[q] = sl;
+              slot_src[perm[q]] = sl;
+            }
+            base += __popc(mask);
           }
         }
       }
@@ -192,6 +250,8 @@ cta_exact_kernel(BatchView bv) {
       if (flags[0]) break;
 
       // ---- 3. the panel's row swaps on the other columns ------------------
+      int tot_new = 0;
+      if (t < P) tot_new = total[perm[t]];
       if (tc != jb) {
 #pragma unroll
         for (int r = 0; r < B; ++r) {
@@ -203,6 +263,7 @@ cta_exact_kernel(BatchView bv) {
         }
       }
       __syncthreads();
+      if (t < P) total[t] = tot_new;
       if (tc != jb) {
 #pragma unroll
         for (int r = 0; r < B; ++r) {
@@ -212,21 +273,28 @@ cta_exact_kernel(BatchView bv) {
             for (int c = 0; c < B; ++c) a[r][c] = Rs[sl * P + col0 + c];
           }
         }
-        // ---- 4. pivot rows at their own step (thread row jb) --------------
+        // ---- 4. pivot rows at their own step (thread row jb), in registers -
         if (tr == jb && (KIND == kInvert || tc > jb)) {
+          // padding rows of a last, partial panel are zero with zero multipliers,
+          // so every loop runs over the full panel width
 #pragma unroll
-          for (int k = 0; k < B; ++k) {
-            if (k < nb) {
+          for (int k = 1; k < B; ++k) {
+            const int org = perm[j0 + k];
+            double mk[B];
 #pragma unroll
-              for (int c = 0; c < B; ++c) {
-                double v = a[k][c];
+            for (int kk = 0; kk < k; ++kk) mk[kk] = Mm[org * PS + kk];
 #pragma unroll
-                for (int kk = 0; kk < k; ++kk)
-                  v = sub_rn(v, mul_rn(Mm[(j0 + k) * PS + kk], Vs[kk * P + col0 + c]));
-                Vs[k * P + col0 + c] = v;
-              }
+            for (int c = 0; c < B; ++c) {
+              double v = a[k][c];
+#pragma unroll
+              for (int kk = 0; kk < k; ++kk) v = sub_rn(v, mul_rn(mk[kk], a[kk][c]));
+              a[k][c] = v;
             }
           }
+#pragma unroll
+          for (int k = 0; k < B; ++k)
+#pragma unroll
+            for (int c = 0; c < B; ++c) Vs[k * P + col0 + c] = a[k][c];
         }
       }
       __syncthreads();
@@ -234,9 +302,11 @@ cta_exact_kernel(BatchView bv) {
       // ---- 5. rank-nb update of this thread's block ------------------------
       if (tc == jb) {
 #pragma unroll
-        for (int r = 0; r < B; ++r)
+        for (int r = 0; r < B; ++r) {
+          const int org = perm[row0 + r];
 #pragma unroll
-          for (int c = 0; c < B; ++c) a[r][c] = Pn[(row0 + r) * PS + c];
+          for (int c = 0; c < B; ++c) a[r][c] = Pn[org * PS + c];
+        }
       } else if (tr == jb) {
         // the panel's pivot rows: their final values from V
         if (KIND == kInvert || tc > jb) {
@@ -247,10 +317,11 @@ cta_exact_kernel(BatchView bv) {
               for (int c = 0; c < B; ++c) {
                 double acc = Vs[k * P + col0 + c];
                 if (KIND == kInvert) {
+                  const int org = perm[j0 + k];
                   acc = acc * rinv_s[k];
 #pragma unroll
                   for (int k2 = k + 1; k2 < B; ++k2)
-                    if (k2 < nb) acc = fma(-Mm[(j0 + k) * PS + k2], Vs[k2 * P + col0 + c], acc);
+                    if (k2 < nb) acc = fma(-Mm[org * PS + k2], Vs[k2 * P + col0 + c], acc);
                 }
                 a[k][c] = acc;
               }
@@ -259,25 +330,36 @@ cta_exact_kernel(BatchView bv) {
         }
       } else {
         const bool lu_region = (tr > jb) && (tc > jb);   // below the panel, right of it
-        if (KIND == kInvert || lu_region) {
+        int org[B];
+#pragma unroll
+        for (int r = 0; r < B; ++r) org[r] = perm[row0 + r];
+        if (lu_region) {
+          // GSL's LU region: one rounding per product and per difference, k ascending
 #pragma unroll
           for (int k = 0; k < B; ++k) {
-            if (k < nb) {
-              double vk[B];
+            double vk[B], mk[B];
 #pragma unroll
-              for (int c = 0; c < B; ++c) vk[c] = Vs[k * P + col0 + c];
+            for (int c = 0; c < B; ++c) vk[c] = Vs[k * P + col0 + c];
 #pragma unroll
-              for (int r = 0; r < B; ++r) {
-                const double m = Mm[(row0 + r) * PS + k];
-                if (lu_region) {
+            for (int r = 0; r < B; ++r) mk[r] = Mm[org[r] * PS + k];
 #pragma unroll
-                  for (int c = 0; c < B; ++c) a[r][c] = sub_rn(a[r][c], mul_rn(m, vk[c]));
-                } else {
+            for (int r = 0; r < B; ++r)
 #pragma unroll
-                  for (int c = 0; c < B; ++c) a[r][c] = fma(-m, vk[c], a[r][c]);
-                }
-              }
-            }
+              for (int c = 0; c < B; ++c) a[r][c] = sub_rn(a[r][c], mul_rn(mk[r], vk[c]));
+          }
+        } else if (KIND == kInvert) {
+          // rows above the panel or columns left of it: outside the LU region
+#pragma unroll
+          for (int k = 0; k < B; ++k) {
+            double vk[B], mk[B];
+#pragma unroll
+            for (int c = 0; c < B; ++c) vk[c] = Vs[k * P + col0 + c];
+#pragma unroll
+            for (int r = 0; r < B; ++r) mk[r] = Mm[org[r] * PS + k];
+#pragma unroll
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+              for (int c = 0; c < B; ++c) a[r][c] = fma(-mk[r], vk[c], a[r][c]);
           }
         }
       }
@@ -294,18 +376,8 @@ cta_exact_kernel(BatchView bv) {
     }
 
     if (KIND == kInvert) {
-      // reverse-order column unscramble: output column perm[k] takes column k
-      if (t == 0) {
-        int* src = slot_src;
-        for (int c = 0; c < n; ++c) src[c] = c;
-        for (int jj = n - 1; jj >= 0; --jj) {
-          const int q = ipiv[jj];
-          if (q != jj) { const int x = src[jj]; src[jj] = src[q]; src[q] = x; }
-        }
-        for (int c = 0; c < n; ++c) perm[src[c]] = c;
-      }
-      __syncthreads();
-      double* __restrict__ Og = bv.out + bv.offA[s];
+      // A^-1 = W P: output column total[i] takes column i of W
+      double* stage = dsm;
 #pragma unroll
       for (int r = 0; r < B; ++r) {
         const int row = row0 + r;
@@ -313,9 +385,16 @@ cta_exact_kernel(BatchView bv) {
 #pragma unroll
           for (int c = 0; c < B; ++c) {
             const int col = col0 + c;
-            if (col < n) Og[int64_t(row) * n + perm[col]] = a[r][c];
+            if (col < n) stage[row * Sh::LS + total[col]] = a[r][c];
           }
         }
+      }
+      __syncthreads();
+      double* __restrict__ Og = bv.out + bv.offA[s];
+#pragma unroll
+      for (int u = 0; u < Sh::PER; ++u) {
+        const int e = t + u * Sh::NT, row = e / P, col = e - (e / P) * P;
+        if (e < P * P && row < n && col < n) Og[int64_t(row) * n + col] = stage[row * Sh::LS + col];
       }
       if (t == 0) {
         bv.status[s] = kOk;
@@ -329,8 +408,8 @@ cta_exact_kernel(BatchView bv) {
       double* vec = dsm + P * LS;
       double* xs = vec + P;
       int* pm = reinterpret_cast<int*>(xs + P);
-      // the pivots sit inside the area the LU copy overwrites: move them first
-      if (t < n) pm[t] = ipiv[t];
+      // GSL's permutation (lu.c:95-109): pm[i] = original row now at i
+      if (t < n) pm[t] = total[t];
       __syncthreads();
 #pragma unroll
       for (int r = 0; r < B; ++r)
@@ -339,18 +418,6 @@ cta_exact_kernel(BatchView bv) {
       __syncthreads();
       if (wid == 0) {
         const int64_t ov = bv.offv[s];
-        // gsl_permutation from the row swaps (lu.c:95-109), built in place of
-        // the pivots: pm[i] = original row now at i
-        if (wl == 0) {
-          int* sw = reinterpret_cast<int*>(vec);   // scratch copy of the pivots
-          for (int i = 0; i < n; ++i) sw[i] = pm[i];
-          for (int i = 0; i < n; ++i) pm[i] = i;
-          for (int i = 0; i < n; ++i) {
-            const int q = sw[i];
-            if (pm[q] != pm[i]) { const int x = pm[q]; pm[q] = pm[i]; pm[i] = x; }
-          }
-        }
-        __syncwarp();
         for (int i = wl; i < n; i += 32) vec[i] = bv.b[ov + pm[i]];
         __syncwarp();
         // forward sweep (unit L), ascending j per entry

@@ -69,9 +69,11 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 
-// GSL multiplier rule (lu.c:162-176).
+// GSL multiplier rule (lu.c:162-176).  The division only runs for a pivot
+// below DBL_MIN; the test is the same for every lane of a step.
 __device__ __forceinline__ double gsl_multiplier(double a, double ujj, double rinv) {
-  return (fabs(ujj) >= kDblMin) ? mul_rn(a, rinv) : div_rn(a, ujj);
+  if (fabs(ujj) >= kDblMin) return mul_rn(a, rinv);
+  return div_rn(a, ujj);
 }
 
 // Pivot key: |a| with NaN mapped to 0 (never strictly greater than the running
