@@ -124,7 +124,8 @@ static KernelSpec cta_spec(int cls) {
 template <int KIND>
 static KernelSpec global_spec(int nmax) {
   KernelSpec k;
-  k.fn = reinterpret_cast<const void*>(&global_exact_kernel<KIND>);
+  k.fn = (global_panel_width(nmax) == 16) ? reinterpret_cast<const void*>(&global_exact_kernel<KIND, 16>)
+                                          : reinterpret_cast<const void*>(&global_exact_kernel<KIND, 8>);
   k.threads = kGThreads;
   k.dyn_smem = global_smem_bytes(nmax);
   return k;
@@ -793,7 +794,8 @@ int solve_matrix_batched_noalloc(int nsys, int nmax, const int* n, const int64_t
   double* scratch = nullptr;
   int rc = noalloc_scratch(&scratch);
   if (rc) return rc;
-  const void* fn = reinterpret_cast<const void*>(&global_exact_kernel<kSolve, true>);
+  static_assert(global_panel_width(kNoAllocMaxN) == 16, "no-allocation path uses the 16-wide panel");
+  const void* fn = reinterpret_cast<const void*>(&global_exact_kernel<kSolve, 16, true>);
   const size_t smem = global_smem_bytes(nmax);
   SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   BatchView v;
