@@ -512,6 +512,17 @@ static Context* ctx() {
   return g_ctx.get();
 }
 
+// page-locked host memory: a copy into it does not block the host
+static bool is_pinned_host(const void* ptr) {
+  if (!ptr) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 static bool is_device_ptr(const void* ptr) {
   if (!ptr) return false;
   cudaPointerAttributes at;
@@ -563,6 +574,10 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
     Pipeline* pl = nullptr;
     rc = c->get_pipeline(kind, nsys, n, offA, kind == kSolve ? offv : nullptr, md, &pl);
     if (rc) return rc;
+    // a device-to-host copy into pageable memory would block the host until the
+    // chunk's kernel finished and stall the upload of the next chunks: such
+    // results are fetched once, after the last chunk
+    const bool out_pinned = is_pinned_host(out), st_pinned = is_pinned_host(status);
     SS_CUDA(cudaEventRecord(c->pipe_ev[0], c->stream));
     for (int i = 0; i < kPipeStreams; ++i) SS_CUDA(cudaStreamWaitEvent(c->pipe[i], c->pipe_ev[0], 0));
     for (size_t k = 0; k < pl->chunks.size(); ++k) {
@@ -574,11 +589,15 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
       double* xo = (kind == kSolve) ? dx + ch.v0 : dx + ch.a0;
       rc = plan_run(ch.plan, dA + ch.a0, db + ch.v0, xo, dst + ch.s0, nullptr, st);
       if (rc) return rc;
-      if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(out + ch.v0, xo, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
-      else SS_CUDA(cudaMemcpyAsync(out + ch.a0, xo, na * sizeof(double), cudaMemcpyDeviceToHost, st));
-      SS_CUDA(cudaMemcpyAsync(status + ch.s0, dst + ch.s0, ns * sizeof(int), cudaMemcpyDeviceToHost, st));
+      if (out_pinned) {
+        if (kind == kSolve) SS_CUDA(cudaMemcpyAsync(out + ch.v0, xo, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+        else SS_CUDA(cudaMemcpyAsync(out + ch.a0, xo, na * sizeof(double), cudaMemcpyDeviceToHost, st));
+      }
+      if (st_pinned) SS_CUDA(cudaMemcpyAsync(status + ch.s0, dst + ch.s0, ns * sizeof(int), cudaMemcpyDeviceToHost, st));
     }
     for (int i = 0; i < kPipeStreams; ++i) SS_CUDA(cudaStreamSynchronize(c->pipe[i]));
+    if (!out_pinned) SS_CUDA(cudaMemcpy(out, dx, kind == kSolve ? bytesV : bytesA, cudaMemcpyDeviceToHost));
+    if (!st_pinned) SS_CUDA(cudaMemcpy(status, dst, sizeof(int) * size_t(nsys), cudaMemcpyDeviceToHost));
     return 0;
   }
   SS_CUDA(cudaMemcpyAsync(dA, A, bytesA, cudaMemcpyHostToDevice, c->stream));
