@@ -39,6 +39,15 @@ L2_BYTES = 126 * 2 ** 20
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 HBM_FALLBACK_GBS = 6650.0
 
+# DRAM traffic of the dominant kernel from the committed ncu captures, as a
+# ratio to its algorithmic bytes (captures of a smaller case are scaled by the
+# systems processed): {config: (size class, traffic / algorithmic bytes, capture)}
+TRAFFIC = {
+    1: ("cta64", 437.4 / 487.7, "profiles/cta_exact_kernel_inverse_8192x61.md"),
+    0: ("small28", 25.0 / 25.66, "profiles/small_exact_kernel_solve_4096x27.md"),
+    3: ("global", 623.7 / 336.0, "profiles/global_exact_kernel_inverse_n129-200.md"),
+}
+
 WORKLOADS = {
     0: "ion-balance solve, 4096 x n=27 (config-0 generator)",
     1: "macro-atom inverse, 8192 x n=61 (config-1 generator)",
@@ -403,8 +412,13 @@ def run_ours(args):
     alg_flops = dom.flops()
     hbm_peak, peak_src = measured_peaks()
     fp64_peak = fp64_peak_tflops(device)
+    traffic, traffic_src = args.traffic, "--traffic"
+    if traffic is None and args.config in TRAFFIC and TRAFFIC[args.config][0] == dc and args.nsys is None:
+        traffic = TRAFFIC[args.config][1] * alg_bytes
+        traffic_src = TRAFFIC[args.config][2]
     roofline = {"bound": "hbm", "achieved": alg_bytes / t_kernel / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                "frac": alg_bytes / t_kernel / 1e9 / hbm_peak, "traffic": args.traffic,
+                "frac": alg_bytes / t_kernel / 1e9 / hbm_peak, "traffic": traffic,
+                "traffic_source": traffic_src if traffic is not None else None,
                 "kernel": kernel_name(dom.kind, dc, dm), "size_class": dc, "launch_s": t_kernel,
                 "bytes_per_launch": alg_bytes, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
     t_roof = max(alg_bytes / (hbm_peak * 1e9), alg_flops / (fp64_peak * 1e12))
