@@ -2,7 +2,7 @@
 //
 // A plan groups the systems of one batch layout into size buckets, each served
 // by one kernel family (kernels_small.cuh for n <= 32, kernels_cta.cuh for
-// n <= 128, kernels_global.cuh above), keeps the layout on the device, and
+// n <= 160, kernels_global.cuh above), keeps the layout on the device, and
 // launches the buckets on forked streams so small and large systems overlap.
 // The drop-in entry points (solve_matrix, invert_matrix) and the host-pointer
 // batched calls run through a per-thread context that caches plans and
@@ -62,7 +62,8 @@ struct KernelSpec {
 
 // size classes of the small family (padded row length NP, lanes per system G)
 static const int kSmallNP[] = {4, 8, 12, 16, 20, 24, 28, 32};
-static const int kCtaP[] = {48, 64, 96, 128};
+static const int kCtaP[] = {48, 64, 96, 128, 160};
+constexpr int kCtaClasses = 5;
 
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
@@ -70,7 +71,7 @@ static int small_class(int n) {
   return -1;
 }
 static int cta_class(int n) {
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < kCtaClasses; ++i)
     if (n <= kCtaP[i]) return i;
   return -1;
 }
@@ -104,17 +105,18 @@ static KernelSpec small_spec(int cls, int mode) {
 template <int KIND>
 static KernelSpec cta_spec(int cls) {
   KernelSpec k;
-#define SS_CTA(I, TG, B)                                                                \
+#define SS_CTA(I, P, NT, RG)                                                            \
   case I:                                                                               \
-    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, TG, B>);               \
-    k.threads = TG * TG;                                                                \
-    k.dyn_smem = CtaShape<KIND, TG, B>::dyn_smem;                                       \
+    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, P, NT, RG>);           \
+    k.threads = NT;                                                                     \
+    k.dyn_smem = CtaShape<KIND, P, NT, RG>::dyn_smem;                                   \
     break;
   switch (cls) {
-    SS_CTA(0, 8, 6)
-    SS_CTA(1, 8, 8)
-    SS_CTA(2, 16, 6)
-    SS_CTA(3, 16, 8)
+    SS_CTA(0, 48, 96, 2)
+    SS_CTA(1, 64, 128, 2)
+    SS_CTA(2, 96, 192, 2)
+    SS_CTA(3, 128, 256, 2)
+    SS_CTA(4, 160, 320, 2)
     default: break;
   }
 #undef SS_CTA
@@ -218,7 +220,7 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   SS_CUDA(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device));
 
   // bucket the systems: key = (family, class); global family sorted by size
-  std::vector<int> small_l[8], cta_l[4], glob_l;
+  std::vector<int> small_l[8], cta_l[kCtaClasses], glob_l;
   for (int s = 0; s < nsys; ++s) {
     const int ns = n[s];
     if (ns < 1 || ns > SIROCCO_MAX_N) {
@@ -263,7 +265,7 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   };
   int rc = 0;
   if (!glob_l.empty() && (rc = add_bucket(kFamGlobal, n[glob_l.front()], glob_l))) return rc;
-  for (int c = 3; c >= 0; --c)
+  for (int c = kCtaClasses - 1; c >= 0; --c)
     if ((rc = add_bucket(kFamCta, c, cta_l[c]))) return rc;
   for (int c = 7; c >= 0; --c)
     if ((rc = add_bucket(kFamSmall, c, small_l[c]))) return rc;
@@ -650,7 +652,7 @@ namespace ss {
 
 // ---------------------------------------------------------- no-allocation --
 // Scratch of solve_matrix_batched_noalloc: one n x n slab per resident CTA of the
-// n > 128 solve kernel, in a file-scope device array instead of cudaMalloc'd
+// global-memory solve kernel, in a file-scope device array instead of cudaMalloc'd
 // memory.  Every GPU that loads this library holds the array until the process
 // exits; every call shares it and overwrites what the previous call left there.
 constexpr int kNoAllocMaxN = SIROCCO_NOALLOC_MAX_N;
