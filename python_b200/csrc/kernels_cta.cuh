@@ -136,14 +136,39 @@ cta_exact_kernel(BatchView bv) {
         }
         bool sing = false;
         int k = 0;
-#pragma unroll 1
+        // Software pipelining: a step updates at once only the column the next
+        // pivot search reads; its other columns are updated at the start of the
+        // next step, while that step's reduction is in flight.  dmode: 0 nothing
+        // pending, 1 subtract dl * dpv, 2 scale by drinv (the pivot row); dpv is
+        // the pending step's pivot row in that step's register frame.
+        int dmode[RPL];
+        double dl[RPL], dpv[B];
+        double drinv = 0.0;
+        int dk = 0;
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) { dmode[i] = 0; dl[i] = 0.0; }
+#pragma unroll
+        for (int c = 0; c < B; ++c) dpv[c] = 0.0;
+        auto apply_pending = [&]() {
+#pragma unroll
+          for (int i = 0; i < RPL; ++i) {
+#pragma unroll
+            for (int c = 2; c < B; ++c) {
+              if (dmode[i] == 1 && (KIND == kInvert || dk + c < B))
+                pr[i][c - 1] = sub_rn(pr[i][c - 1], mul_rn(dl[i], dpv[c]));
+              if (KIND == kInvert && dmode[i] == 2) pr[i][c - 1] = mul_rn(pr[i][c - 1], drinv);
+            }
+            dmode[i] = 0;
+          }
+        };
+#pragma unroll 2
         for (; k < nb; ++k) {
           const int j = j0 + k;
           // this lane's best candidate: larger |a| first, then smaller position;
           // eligible rows carry bit 63, NaN counts as zero (cblas idamax)
           unsigned long long kb = 0ull;
           unsigned pb = 0xffffffffu;
-          double vb = 0.0;
+          double vb = 1.0;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
             const int r = wl + 32 * i;
@@ -160,6 +185,7 @@ cta_exact_kernel(BatchView bv) {
           const unsigned mh = __reduce_max_sync(FULL, hi);
           const unsigned ml = __reduce_max_sync(FULL, hi == mh ? lo : 0u);
           const int ppos = int(__reduce_min_sync(FULL, (hi == mh && lo == ml) ? pb : 0xffffffffu));
+          apply_pending();
           int pi = 0;
           bool own = false;
 #pragma unroll
@@ -182,30 +208,37 @@ cta_exact_kernel(BatchView bv) {
           const double rinv = __shfl_sync(FULL, rb, pl);   // = fl(1/u_jj), correctly rounded
           const double ujj = pv[0];
           if (__any_sync(FULL, ujj == 0.0)) { sing = true; break; }
-          const bool tiny = __any_sync(FULL, !(fabs(ujj) >= kDblMin));
+          double lrow[RPL];
+#pragma unroll
+          for (int i = 0; i < RPL; ++i) lrow[i] = mul_rn(pr[i][0], rinv);
+          if (!(fabs(ujj) >= kDblMin)) {
+            // GSL divides by a pivot below DBL_MIN instead of scaling (lu.c:170-176)
+#pragma unroll
+            for (int i = 0; i < RPL; ++i)
+              if (ps[i] > j) lrow[i] = div_rn(pr[i][0], ujj);
+          }
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
             const int r = wl + 32 * i;
             const bool is_piv = (ps[i] == j);
             const bool below = ps[i] > j;
-            if (r < n && !is_piv && (KIND == kInvert || below)) {
-              double l;
-              if (tiny) l = below ? div_rn(pr[i][0], ujj) : mul_rn(pr[i][0], rinv);
-              else l = mul_rn(pr[i][0], rinv);
-              Mm[r * MS + k] = l;
-#pragma unroll
-              for (int c = 1; c < B; ++c) {
-                if (KIND == kSolve && k + c >= B) continue;   // L part of the panel
-                pr[i][c] = sub_rn(pr[i][c], mul_rn(l, pv[c]));
-              }
-              pr[i][0] = (KIND == kInvert) ? -l : l;
+            const bool upd = r < n && !is_piv && (KIND == kInvert || below);
+            dmode[i] = upd ? 1 : ((KIND == kInvert && is_piv) ? 2 : 0);
+            dl[i] = lrow[i];
+            if (upd) {
+              Mm[r * MS + k] = lrow[i];
+              if (KIND == kInvert || k + 1 < B) pr[i][1] = sub_rn(pr[i][1], mul_rn(lrow[i], pv[1]));
+              pr[i][0] = (KIND == kInvert) ? -lrow[i] : lrow[i];
             }
             if (KIND == kInvert && is_piv) {
               pr[i][0] = rinv;
-#pragma unroll
-              for (int c = 1; c < B; ++c) pr[i][c] = mul_rn(pr[i][c], rinv);
+              pr[i][1] = mul_rn(pr[i][1], rinv);
             }
           }
+#pragma unroll
+          for (int c = 0; c < B; ++c) dpv[c] = pv[c];
+          drinv = rinv;
+          dk = k;
           if (wl == 0) rinv_s[k] = rinv;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
@@ -215,6 +248,7 @@ cta_exact_kernel(BatchView bv) {
             pr[i][B - 1] = first;
           }
         }
+        if (!sing) apply_pending();
         if (sing) {
           if (wl == 0) flags[0] = 1;
         } else {
