@@ -9,6 +9,12 @@ macro-atom jumping matrices of order 61 inverted (invert_matrix).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config 0|1|3|4]
     python bench.py --impl reference ...   # the reference's CPU path, all host cores
 
+Beside the engine's numbers the line reports the reference's own CPU path
+(``cpu_baseline``: source/matrix_cpu.c + GSL, every host core) and the
+reference's cuSOLVER build (``cusolver_reference``: source/matrix_gpu.cu, one
+call per system as its CUDA_ON build makes them), each timed on a bounded
+sample of the same workload outside the timed region.
+
 The path does not shard with an exchange step: with N > 1 (torchrun) every rank
 runs an independent replica of the workload ("replicas only", weak scaling);
 ``value`` is the systems of all ranks over the slowest rank's device time.
@@ -214,6 +220,53 @@ def cpu_reference_run(batch: wl.Batch, threads: int, seconds: float, seed: int =
                       f"one serial {'solve_matrix' if batch.kind == 'solve' else 'invert_matrix'} call per "
                       f"system on a fresh copy of A"}
     return reps * sample.nsys / dt, info
+
+
+def cusolver_reference_run(batch: wl.Batch, seconds: float, seed: int = 0):
+    """Time the reference's cuSOLVER build (source/matrix_gpu.cu, one
+    gpu_solve_matrix / gpu_invert_matrix call per system, each allocating,
+    copying and freeing) on a bounded sample; returns (systems/s, info) or
+    (None, reason)."""
+    from oracle import oracle
+    if not oracle.cusolver_available():
+        return None, "reference cuSOLVER build not present (oracle/_ref/libref_cusolver.so)"
+    rng = np.random.default_rng(seed)
+    fn = oracle.cusolver_solve if batch.kind == "solve" else oracle.cusolver_invert
+    probe = subset(batch, rng.choice(batch.nsys, size=min(8, batch.nsys), replace=False))
+    fn(probe)                                    # handle creation, first-call costs
+    t0 = time.perf_counter()
+    fn(probe)
+    per_sys = max((time.perf_counter() - t0) / probe.nsys, 1e-6)
+    size = int(min(batch.nsys, max(16, seconds / per_sys)))
+    idx = np.sort(rng.choice(batch.nsys, size=size, replace=False))
+    sample = subset(batch, idx)
+    t0 = time.perf_counter()
+    out, st = fn(sample)
+    dt = time.perf_counter() - t0
+    # agreement with the GSL path on the same sample, for information
+    from oracle import oracle as orc
+    if batch.kind == "solve":
+        ref, sr = orc.solve(sample, "port", threads=orc.host_threads())
+        ok = sr != 4
+        worst = 0.0
+        for j in np.nonzero(ok)[0]:
+            a, b = int(sample.offv[j]), int(sample.offv[j]) + int(sample.n[j])
+            r, v = ref[a:b], out[a:b]
+            sig = np.abs(r) > 1e-20 * np.abs(r).sum()
+            if sig.any():
+                worst = max(worst, float(np.max(np.abs(v[sig] - r[sig]) / np.abs(r[sig]))))
+    else:
+        ref, sr = orc.invert(sample, "port", threads=orc.host_threads())
+        worst = 0.0
+        for j in np.nonzero(sr == 0)[0]:
+            a, b = int(sample.offA[j]), int(sample.offA[j]) + int(sample.n[j]) ** 2
+            worst = max(worst, float(np.max(np.abs(out[a:b] - ref[a:b])) / np.max(np.abs(ref[a:b]))))
+    info = {"value": size / dt, "unit": UNIT,
+            "sample": f"{size} (random, seeded) of {batch.nsys} systems, {dt:.2f} s wall, one "
+                      f"{'gpu_solve_matrix' if batch.kind == 'solve' else 'gpu_invert_matrix'} call per system "
+                      f"from host memory (the reference's CUDA_ON build, cusolverDnDgetrf/getrs)",
+            "max_rel_err_vs_gsl": worst}
+    return size / dt, info
 
 
 def run_reference(args):
@@ -480,6 +533,21 @@ def run_ours(args):
         cpu["value"] = nsys_step / t_sys
         cpu["unit"] = UNIT
 
+    # the reference's own GPU path (its cuSOLVER build), timed on a bounded sample
+    cus = None
+    if rank == 0 and world == 1 and not args.no_cusolver:
+        t_sys, infos = 0.0, []
+        for b in batches:
+            r, info = cusolver_reference_run(b, args.cusolver_seconds / len(batches))
+            if r is None:
+                cus = {"unavailable": info}
+                break
+            t_sys += b.nsys / r
+            infos.append(info)
+        if cus is None:
+            cus = {"value": nsys_step / t_sys, "unit": UNIT, "sample": " + ".join(i["sample"] for i in infos),
+                   "max_rel_err_vs_gsl": max(i["max_rel_err_vs_gsl"] for i in infos)}
+
     # plain FP64 batched kernel on the same workload, for the mixed-vs-FP64 ratio
     fp64_value = None
     if any(m == "mixed" for m in modes):
@@ -514,7 +582,7 @@ def run_ours(args):
                 "accuracy": acc, "plain_fp64_value": fp64_value,
                 "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
                 "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clock_info}
+                "cusolver_reference": cus, "gpu_launches": launches, "clocks": clock_info}
         print(json.dumps(line), flush=True)
     for p in plans:
         p.close()
@@ -536,6 +604,9 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cusolver", action="store_true",
+                    help="skip timing the reference's cuSOLVER build")
+    ap.add_argument("--cusolver-seconds", type=float, default=5.0)
     ap.add_argument("--ref-seconds", type=float, default=120.0)
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the dominant kernel from an ncu capture")
