@@ -57,6 +57,7 @@ TRAFFIC = {
 WORKLOADS = {
     0: "ion-balance solve, 4096 x n=27 (config-0 generator)",
     1: "macro-atom inverse, 8192 x n=61 (config-1 generator)",
+    2: "conditioning sweep: log10 kappa_2 in {2,4,6,8,10,12} x 2048 systems, ion n=27 solves and macro n=61 inverses",
     3: "50k cells: 10 ion solves n in {2..27} + 1 macro inverse n~U[20,200] per cell, shuffled",
     4: "large macro inverse, 2048 x n~U[256,1024], 10% nonzero",
 }
@@ -68,6 +69,8 @@ def make_batches(config: int, nsys: int | None = None):
         return [wl.config0(nsys=nsys or 4096)]
     if config == 1:
         return [wl.config1(nsys=nsys or 8192)]
+    if config == 2:
+        raise SystemExit("config 2 is the conditioning sweep (bench.py --config 2), not a throughput workload")
     if config == 3:
         s, i = wl.config3(ncells=nsys or 50_000)
         return [s, i]
@@ -591,6 +594,118 @@ def run_ours(args):
     return 0
 
 
+def run_sweep(args):
+    """Config 2: the conditioning sweep.  Per generator and log10 kappa_2 group,
+    the mixed path (equilibrated FP32 LU + FP64 refinement, solves n <= 32)
+    against the plain FP64 path on the GPU: forward and backward error,
+    refinement steps, fallback fraction and throughput of both."""
+    import torch
+
+    from python_b200 import engine
+    rank, world, local = dist_env()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    engine.load()
+    nsys = args.nsys or 2048
+    stream = torch.cuda.current_stream(device)
+    groups, mixed_rate, fp64_rate = [], [], []
+
+    def timed(plan, A, out, st, b, diag):
+        for _ in range(args.warmup):
+            plan.execute(A, out, st, b=b, diag=diag, stream=stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(A, out, st, b=b, diag=diag, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return e0.elapsed_time(e1) / 1e3 / args.steps
+
+    for gen in ("ion", "macro"):
+        for lk in wl.KAPPA_GROUPS:
+            batch, kap, reachable = wl.config2(gen, lk, nsys=nsys)
+            A = torch.from_numpy(batch.A).to(device)
+            b = torch.from_numpy(batch.b).to(device) if batch.kind == "solve" else None
+            size = batch.b.size if batch.kind == "solve" else batch.A.size
+            res = {"generator": gen, "kind": batch.kind, "log10_kappa_target": lk, "systems": batch.nsys,
+                   "log10_kappa": {"min": float(kap.min()), "median": float(np.median(kap)), "max": float(kap.max())},
+                   "target_band_reachable": reachable}
+            outs = {}
+            for mode in ("fp64", "mixed"):
+                if mode == "mixed" and batch.kind != "solve":
+                    res["mixed"] = "not built: a refined inverse needs the FP64 residual I - A X, as many FP64 flops as the FP64 inverse"
+                    continue
+                plan = engine.Plan(batch, engine.FP64 if mode == "fp64" else engine.MIXED)
+                out = torch.empty(size, dtype=torch.float64, device=device)
+                st = torch.empty(batch.nsys, dtype=torch.int32, device=device)
+                diag = torch.zeros(batch.nsys, dtype=torch.int32, device=device)
+                dt = timed(plan, A, out, st, b, diag)
+                plan.close()
+                outs[mode] = (out.cpu().numpy(), st.cpu().numpy(), diag.cpu().numpy(), batch.nsys / dt)
+            # host-side error analysis (FP64 arithmetic, numpy)
+            n = int(batch.n[0])
+            M = batch.A.reshape(batch.nsys, n, n)
+            xf, sf, _, rf = outs["fp64"]
+            res["fp64"] = {"systems_per_s": rf, "singular": int(np.sum(sf == (4 if batch.kind == "solve" else 1)))}
+            fp64_rate.append(rf)
+            if batch.kind == "solve":
+                B = batch.b.reshape(batch.nsys, n)
+                XF = xf.reshape(batch.nsys, n)
+
+                def backward(X):
+                    r = np.abs(B - np.einsum("sij,sj->si", M, X)).max(axis=1)
+                    return r / (np.abs(M).sum(axis=2).max(axis=1) * np.abs(X).max(axis=1))
+                ok = sf != 4
+                res["fp64"]["backward_err"] = {"median": float(np.median(backward(XF)[ok])), "max": float(backward(XF)[ok].max())}
+                xm, sm, dm, rm = outs["mixed"]
+                XM = xm.reshape(batch.nsys, n)
+                fb = (dm & 0x100) != 0
+                acc = ok & ~fb
+                fwd = np.zeros(batch.nsys)
+                for i in np.nonzero(ok)[0]:
+                    sig = np.abs(XF[i]) > 1e-20 * np.abs(XF[i]).sum()
+                    fwd[i] = np.max(np.abs(XM[i][sig] - XF[i][sig]) / np.abs(XF[i][sig])) if sig.any() else 0.0
+                it = dm & 0xff
+                res["mixed"] = {"systems_per_s": rm, "fallback_frac": float(fb.mean()),
+                                "codes_match_fp64": bool(np.array_equal(sm, sf)),
+                                "forward_err_vs_fp64": {"median_accepted": float(np.median(fwd[acc])) if acc.any() else None,
+                                                        "max_accepted": float(fwd[acc].max()) if acc.any() else None,
+                                                        "max_all": float(fwd[ok].max()) if ok.any() else None},
+                                "backward_err": {"median": float(np.median(backward(XM)[ok])), "max": float(backward(XM)[ok].max())},
+                                "refinement_steps": {"mean_accepted": float(it[acc].mean()) if acc.any() else None,
+                                                     "max_accepted": int(it[acc].max()) if acc.any() else None}}
+                mixed_rate.append(rm)
+            else:
+                XF = xf.reshape(batch.nsys, n, n)
+                ok = sf == 0
+                eye = np.eye(n)
+                R = np.abs(eye - np.einsum("sij,sjk->sik", M, XF)).sum(axis=2).max(axis=1)
+                bwd = R / (np.abs(M).sum(axis=2).max(axis=1) * np.abs(XF).sum(axis=2).max(axis=1))
+                res["fp64"]["backward_err"] = {"median": float(np.median(bwd[ok])), "max": float(bwd[ok].max())}
+                from oracle import oracle
+                idx = np.arange(0, batch.nsys, max(1, batch.nsys // 256))
+                sub = subset(batch, idx)
+                ir, sr = oracle.invert(sub, "port", threads=oracle.host_threads())
+                worst = 0.0
+                for j, s_ in enumerate(idx):
+                    if sr[j] == 0:
+                        r = ir[sub.offA[j]:sub.offA[j] + n * n]
+                        v = xf[batch.offA[s_]:batch.offA[s_] + n * n]
+                        worst = max(worst, float(np.max(np.abs(v - r)) / np.max(np.abs(r))))
+                res["fp64"]["max_rel_err_vs_gsl_sample"] = worst
+            groups.append(res)
+    if rank == 0:
+        value = float(np.sum([nsys for _ in mixed_rate]) / np.sum([nsys / r for r in mixed_rate])) if mixed_rate else None
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic (config-0 / config-1 generators, rate spread widened per kappa group, rejection-sampled)",
+                "config": {"workload": WORKLOADS[2], "config_index": 2, "systems_per_group": nsys},
+                "value_is": "mixed-mode solve throughput over the ion groups (harmonic mean)",
+                "sweep": groups}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -615,6 +730,8 @@ def main(argv=None):
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == 2:
+        return run_sweep(args)
     return run_ours(args)
 
 

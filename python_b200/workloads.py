@@ -143,6 +143,59 @@ def config1(nsys=8192, n=61, seed=BASE_SEED + 1) -> Batch:
     return _pack("invert", [macro_matrix(rng, n) for _ in range(nsys)])
 
 
+KAPPA_GROUPS = (2, 4, 6, 8, 10, 12)
+# ion-chain rate spreads (decades below 1e2) whose draws land near each target
+# log10 kappa_2 for order 27; the chain's own spectrum keeps kappa_2 above
+# ~10^2.6 at this order, so the lowest group takes the narrowest spread
+_ION_DECADES = {2: (0.0, 0.0), 4: (0.5, 2.5), 6: (1.5, 4.5), 8: (2.5, 6.5), 10: (3.0, 8.5), 12: (4.0, 10.0)}
+
+
+def config2(generator: str, log_kappa: int, nsys: int = 2048, seed: int = BASE_SEED + 2, tol: float = 0.5):
+    """One group of the conditioning sweep.
+
+    ``generator`` "ion" (config-0 systems, order 27, solved) or "macro"
+    (config-1 matrices, order 61, inverted) with the rate spread widened until
+    log10 kappa_2 = ``log_kappa`` +- ``tol`` (kappa_2 from an FP64 SVD on the
+    host, rejection-sampled).  Returns (batch, log10 kappa_2 per system,
+    whether the target band was reachable).
+    """
+    rng = np.random.default_rng([seed, log_kappa, 0 if generator == "ion" else 1])
+    mats, rhs, kap = [], [], []
+    reachable = True
+    if generator == "ion":
+        lo, hi = _ION_DECADES[log_kappa]
+        tries = 0
+        budget = 4 * nsys if hi == 0.0 else 200 * nsys
+        while len(mats) < nsys and tries < budget:
+            cand = []
+            for _ in range(256):
+                d = rng.uniform(lo, hi)
+                cand.append(ion_matrix(rng, 27, spread=(10.0 ** (2.0 - d), 1e2)))
+            tries += 256
+            k = np.log10(np.linalg.cond(np.stack([a for a, _ in cand])))
+            for (a, b), kk in zip(cand, k):
+                if abs(kk - log_kappa) <= tol and len(mats) < nsys:
+                    mats.append(a), rhs.append(b), kap.append(kk)
+        if len(mats) < nsys:
+            # band below what the chain allows: keep the best-conditioned draws
+            reachable = False
+            need = nsys - len(mats)
+            cand = [ion_matrix(rng, 27, spread=(1e2, 1e2)) for _ in range(need)]
+            k = np.log10(np.linalg.cond(np.stack([a for a, _ in cand])))
+            for (a, b), kk in zip(cand, k):
+                mats.append(a), rhs.append(b), kap.append(kk)
+        return _pack("solve", mats, rhs), np.array(kap), reachable
+    # macro: kappa_2 follows the smallest deactivation probability (no absorbing rows)
+    t = log_kappa - 0.27
+    while len(mats) < nsys:
+        cand = [macro_matrix(rng, 61, pdeact=(10.0 ** (-t), 2 * 10.0 ** (-t)), identity_frac=0.0) for _ in range(64)]
+        k = np.log10(np.linalg.cond(np.stack(cand)))
+        for m, kk in zip(cand, k):
+            if abs(kk - log_kappa) <= tol and len(mats) < nsys:
+                mats.append(m), kap.append(kk)
+    return _pack("invert", mats), np.array(kap), reachable
+
+
 def config3(ncells=50_000, seed=BASE_SEED + 3, macro_range=(20, 200)):
     """Mixed-size batch: per cell 10 ion systems (orders ION_SIZES_PER_CELL)
     and one macro-atom inverse of order uniform in ``macro_range``; the order
