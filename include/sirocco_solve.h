@@ -71,7 +71,7 @@ int gpu_invert_matrix(double *matrix, double *inverse, int num_rows);
 #define SIROCCO_EINVAL (-1)   /* bad argument: nsys < 0, n < 1, null pointer   */
 #define SIROCCO_ESIZE (-2)    /* a system larger than the engine supports      */
 #define SIROCCO_EMODE (-3)    /* unknown precision mode                        */
-#define SIROCCO_MAX_N 1024  /* shared-memory bound of the n > 160 path */
+#define SIROCCO_MAX_N 1024  /* shared-memory bound of the n > 256 path */
 
 /* Batched solve, called once per ionisation cycle (or once per n_e round of
    the lock-step ion iteration) over all cells' systems.  The layout arrays

@@ -2,7 +2,7 @@
 //
 // A plan groups the systems of one batch layout into size buckets, each served
 // by one kernel family (kernels_small.cuh for n <= 32, kernels_cta.cuh for
-// n <= 160, kernels_global.cuh above), keeps the layout on the device, and
+// n <= 256, kernels_global.cuh above), keeps the layout on the device, and
 // launches the buckets on forked streams so small and large systems overlap.
 // The drop-in entry points (solve_matrix, invert_matrix) and the host-pointer
 // batched calls run through a per-thread context that caches plans and
@@ -58,12 +58,13 @@ struct KernelSpec {
   size_t dyn_smem = 0;
   int sys_per_block = 1;
   int blocks_per_sm = 1;
+  int64_t work_slab = 0;   // CTA family with the matrix in global memory: doubles per CTA
 };
 
 // size classes of the small family (padded row length NP, lanes per system G)
 static const int kSmallNP[] = {4, 8, 12, 16, 20, 24, 28, 32};
-static const int kCtaP[] = {48, 64, 96, 128, 160};
-constexpr int kCtaClasses = 5;
+static const int kCtaP[] = {48, 64, 96, 128, 160, 192, 224, 256};
+constexpr int kCtaClasses = 8;
 
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
@@ -105,18 +106,26 @@ static KernelSpec small_spec(int cls, int mode) {
 template <int KIND>
 static KernelSpec cta_spec(int cls) {
   KernelSpec k;
-#define SS_CTA(I, P, NT, RG)                                                            \
-  case I:                                                                               \
-    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, P, NT, RG>);           \
+#define SS_CTA(I, P, NT, RG, CC, PW, GM, MINB)                                          \
+  case I: {                                                                             \
+    using Sh = CtaShape<KIND, P, NT, RG, CC, PW, GM, MINB>;                             \
+    k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, P, NT, RG, CC, PW, GM, MINB>); \
     k.threads = NT;                                                                     \
-    k.dyn_smem = CtaShape<KIND, P, NT, RG>::dyn_smem;                                   \
-    break;
+    k.dyn_smem = Sh::dyn_smem;                                                          \
+    k.work_slab = Sh::slab;                                                             \
+    break;                                                                              \
+  }
+  // order classes up to 160 keep the matrix in shared memory; above, in a
+  // global workspace slab per CTA with two panel warps
   switch (cls) {
-    SS_CTA(0, 48, 96, 2)
-    SS_CTA(1, 64, 128, 2)
-    SS_CTA(2, 96, 192, 2)
-    SS_CTA(3, 128, 256, 2)
-    SS_CTA(4, 160, 320, 2)
+    SS_CTA(0, 48, 96, 2, 6, 1, false, 0)
+    SS_CTA(1, 64, 128, 2, 8, 1, false, 0)
+    SS_CTA(2, 96, 192, 2, 12, 1, false, 0)
+    SS_CTA(3, 128, 256, 2, 16, 1, false, 0)
+    SS_CTA(4, 160, 320, 2, 20, 1, false, 0)
+    SS_CTA(5, 192, 256, 2, 8, 3, true, 2)
+    SS_CTA(6, 224, 224, 2, 7, 4, true, 2)
+    SS_CTA(7, 256, 256, 2, 8, 4, true, 2)
     default: break;
   }
 #undef SS_CTA
@@ -158,7 +167,7 @@ struct Bucket {
   int list_off;
   KernelSpec spec;
   int grid;
-  int64_t slab;   // global family, solve: scratch elements per CTA
+  int64_t slab;   // scratch elements per CTA (global solves, CTA classes in global memory)
   int64_t scratch_off;
 };
 
@@ -260,6 +269,11 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
       b.scratch_off = scratch_elems;
       scratch_elems += b.slab * b.grid;
     }
+    if (fam == kFamCta && b.spec.work_slab > 0) {
+      b.slab = b.spec.work_slab;
+      b.scratch_off = scratch_elems;
+      scratch_elems += b.slab * b.grid;
+    }
     p->buckets.push_back(b);
     return 0;
   };
@@ -315,6 +329,10 @@ static int launch_bucket(const sirocco_plan* p, const Bucket& b, const double* A
     double* scratch = p->d_scratch ? p->d_scratch + b.scratch_off : nullptr;
     int64_t slab = b.slab;
     void* args[] = {&v, &nmax, &scratch, &slab};
+    SS_CUDA(cudaLaunchKernel(b.spec.fn, dim3(b.grid), dim3(b.spec.threads), args, b.spec.dyn_smem, st));
+  } else if (b.fam == kFamCta) {
+    double* work = (b.slab > 0 && p->d_scratch) ? p->d_scratch + b.scratch_off : nullptr;
+    void* args[] = {&v, &work};
     SS_CUDA(cudaLaunchKernel(b.spec.fn, dim3(b.grid), dim3(b.spec.threads), args, b.spec.dyn_smem, st));
   } else if (b.fam == kFamSmall && p->mode == SIROCCO_MIXED && p->kind == kSolve) {
     MixedParams mp = default_mixed_params();

@@ -1,15 +1,18 @@
-// CTA-per-system kernels for 32 < n <= 160 (macro-atom jumping matrices of a
-// few dozen to ~160 levels, per-element macro populations).
+// CTA-per-system kernels for 32 < n <= 256 (macro-atom jumping matrices of a
+// few dozen to a few hundred levels, per-element macro populations).
 //
-// The padded P x P matrix stays in shared memory for the whole factorisation
-// (row-major, columns XOR-swizzled inside 16-column groups so that row, column
-// and tile accesses are all free of bank conflicts).  Rows never move: each
-// physical row carries its current position (ps), and perm[q] names the row
-// at position q, so GSL's row swaps cost two integer stores and ties in the
-// pivot search break on positions exactly as GSL's physical swaps would.
-// The factorisation is blocked by panels of B = 8 columns.  Per panel:
-//   1. warp 0 factorises the n x B panel in its registers (GSL's LU_decomp_L2
-//      on a panel, lu.c:129-191): first strict maximum pivot by a three-step
+// The padded P x P matrix is held row-major with its columns XOR-swizzled
+// inside 16-column groups (row, column and tile accesses are then free of
+// shared-memory bank conflicts and stay inside one 128-byte line): in shared
+// memory for P <= 160, in an L2-resident global workspace slab per CTA above
+// that, where several CTAs per SM keep several pivot chains in flight.  Rows
+// never move: each physical row carries its current position (ps), and
+// perm[q] names the row at position q, so GSL's row swaps cost two integer
+// stores and ties in the pivot search break on positions exactly as GSL's
+// physical swaps would.  The factorisation is blocked by panels of B = 8
+// columns.  Per panel:
+//   1. the panel warps factorise the n x B panel in registers (GSL's
+//      LU_decomp_L2 on a panel, lu.c:129-191): first strict maximum pivot by a
 //      warp reduction of (|a|, position), multipliers a * fl(1/u) (a / u below
 //      DBL_MIN), one rounding per product and per difference; every row's
 //      multipliers are recorded (Mm);
@@ -38,51 +41,68 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// barrier 1 over the first `count` threads (the panel warps)
+__device__ __forceinline__ void panel_bar(int count) { asm volatile("bar.sync 1, %0;\n" ::"r"(count) : "memory"); }
+
 constexpr int kSmemPerSm = 233472;   // shared memory of one SM (228 KB)
 
-template <int KIND, int P_, int NT_, int RG_>
+// P: padded order; NT: threads; RG x CC: rows x columns of one update tile
+// (columns tc + 8c); PW: panel warps; GM: matrix in a global workspace slab;
+// MINB: CTAs per SM asked of the register allocator (0: as many as fit).
+template <int KIND, int P_, int NT_, int RG_, int CC_, int PW_, bool GM_, int MINB_>
 struct CtaShape {
-  static constexpr int P = P_;             // padded order
-  static constexpr int NT = NT_;           // threads
+  static constexpr int P = P_;
+  static constexpr int NT = NT_;
+  static constexpr int NW = NT / 32;
   static constexpr int B = 8;              // panel width
   static constexpr int TGC = 8;            // thread columns of the update tiling
   static constexpr int TGR = NT / TGC;     // thread rows
   static constexpr int CB = P / TGC;       // columns per thread (tc + 8 c)
   static constexpr int RB = P / TGR;       // rows per thread (tr + TGR r)
-  static constexpr int RG = RG_;           // rows updated together
-  static constexpr int RPL = (P + 31) / 32;   // panel rows per lane of warp 0
+  static constexpr int RG = RG_;
+  static constexpr int CC = CC_;
+  static constexpr int PW = PW_;
+  static constexpr int PT = 32 * PW;       // panel threads
+  static constexpr int RPL = (P + PT - 1) / PT;   // panel rows per panel thread
+  static constexpr bool GM = GM_;
   static constexpr int MS = B + 1;         // multiplier row stride (odd)
-  static constexpr int off_Mm = P * P;
+  static constexpr int off_Mm = GM ? 0 : P * P;
   static constexpr int off_V = off_Mm + P * MS;
   static constexpr int off_r = off_V + B * P;
-  static constexpr int n_dbl = off_r + B;
-  static constexpr int n_int = 2 * P + 4;
+  static constexpr int off_pb = off_r + B; // pivot-row exchange of a multi-warp panel
+  static constexpr int n_dbl = off_pb + B + 2;
+  static constexpr int n_int = 2 * P + 4 + 4 * PW;
   static constexpr size_t dyn_smem = size_t(n_dbl) * 8 + size_t(n_int) * 4;
   static constexpr int by_smem = int(kSmemPerSm / (dyn_smem + 1024));
   static constexpr int by_thr = 2048 / NT;
   static constexpr int min_blocks0 = by_smem < by_thr ? by_smem : by_thr;
-  static constexpr int min_blocks = min_blocks0 < 1 ? 1 : min_blocks0;
+  static constexpr int min_blocks1 = (MINB_ > 0 && MINB_ < min_blocks0) ? MINB_ : min_blocks0;
+  static constexpr int min_blocks = min_blocks1 < 1 ? 1 : min_blocks1;
+  static constexpr int64_t slab = GM ? int64_t(P) * P : 0;   // workspace doubles per CTA
   static_assert(P % 16 == 0, "swizzle works on 16-column groups");
   static_assert(NT % 32 == 0 && TGR % 4 == 0, "4 thread rows x 8 thread columns per warp");
-  static_assert(P % TGR == 0 && RB % RG == 0, "whole row groups");
-  static_assert(NT >= P && NT % P == 0, "one thread per column in the pivot-row phase and the copies");
+  static_assert(P % TGR == 0 && RB % RG == 0 && CB % CC == 0, "whole update tiles");
+  static_assert(PW >= 1 && PW <= NW, "panel warps are warps of the CTA");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
 };
 
-template <int KIND, int P, int NT, int RG>
-__global__ void __launch_bounds__(NT, (CtaShape<KIND, P, NT, RG>::min_blocks))
-cta_exact_kernel(BatchView bv) {
-  using Sh = CtaShape<KIND, P, NT, RG>;
+template <int KIND, int P, int NT, int RG, int CC, int PW, bool GM, int MINB>
+__global__ void __launch_bounds__(NT, (CtaShape<KIND, P, NT, RG, CC, PW, GM, MINB>::min_blocks))
+cta_exact_kernel(BatchView bv, double* __restrict__ work) {
+  using Sh = CtaShape<KIND, P, NT, RG, CC, PW, GM, MINB>;
   constexpr int B = Sh::B, MS = Sh::MS, CB = Sh::CB, TGR = Sh::TGR, RB = Sh::RB, RPL = Sh::RPL;
+  constexpr int PT = Sh::PT, NW = Sh::NW;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) double dsm[];
-  double* M = dsm;                         // [P][P] the matrix, swizzled
+  double* M = GM ? work + int64_t(blockIdx.x) * Sh::slab : dsm;   // [P][P] the matrix, swizzled
   double* Mm = dsm + Sh::off_Mm;           // [P][MS] multipliers of this panel, by row
   double* Vs = dsm + Sh::off_V;            // [B][P] pivot rows at their own step
   double* rinv_s = dsm + Sh::off_r;        // [B] fl(1/u) of this panel's pivots
+  double* pivbuf = dsm + Sh::off_pb;       // [B+1] pivot row and its reciprocal (PW > 1)
   int* ps_s = reinterpret_cast<int*>(dsm + Sh::n_dbl);   // [P] position of each row
   int* perm = ps_s + P;                    // [P] row at each position
   int* flags = perm + P;                   // [0] singular
+  unsigned* cand = reinterpret_cast<unsigned*>(flags + 4);   // [PW][4] per-warp pivot candidates
 
   const int t = threadIdx.x;
   const int wid = t >> 5, wl = t & 31;
@@ -93,19 +113,23 @@ cta_exact_kernel(BatchView bv) {
     const int n = bv.n[s];
     const double* __restrict__ Ag = bv.A + bv.offA[s];
 
-    // ---- load: rows < n straight into the swizzled layout, padding columns zeroed
-    {
-      const int col = t % P;
-      for (int row = t / P; row < n; row += NT / P) {
-        double* dst = M + row * P + (col ^ cta_swz(row));
-        if (col < n) cp_async8(dst, Ag + int64_t(row) * n + col);
+    // ---- load: rows < n into the swizzled layout, padding columns zeroed; a
+    // warp per row, consecutive lanes on consecutive columns
+    for (int row = wid; row < n; row += NW) {
+      const int sw = cta_swz(row);
+      const double* __restrict__ src = Ag + int64_t(row) * n;
+#pragma unroll 4
+      for (int col = wl; col < P; col += 32) {
+        double* dst = M + row * P + (col ^ sw);
+        if (GM) *dst = (col < n) ? __ldg(src + col) : 0.0;
+        else if (col < n) cp_async8(dst, src + col);
         else *dst = 0.0;
       }
-      if (t < P) { ps_s[t] = t; perm[t] = t; }
-      if (t == 0) flags[0] = 0;
-      cp_async_wait_all();
-      __syncthreads();
     }
+    for (int r = t; r < P; r += NT) { ps_s[r] = r; perm[r] = r; }
+    if (t == 0) flags[0] = 0;
+    if (!GM) cp_async_wait_all();
+    __syncthreads();
 
     const int npan = (n + B - 1) / B;
     bool singular = false;
@@ -113,16 +137,16 @@ cta_exact_kernel(BatchView bv) {
       const int j0 = jb * B;
       const int nb = min(B, n - j0);
 
-      // ---- 1. warp 0 factorises the panel in its registers -------------------
-      // Lane l holds rows l, l+32, ...; the panel is kept rotated so that the
-      // current pivot column is always register column 0.
-      if (wid == 0) {
+      // ---- 1. the panel warps factorise the panel in their registers ----------
+      // Panel thread p holds rows p, p + PT, ...; the panel is kept rotated so
+      // that the current pivot column is always register column 0.
+      if (wid < PW) {
         double pr[RPL][B];
         int ps[RPL];
 #pragma unroll
         for (int i = 0; i < RPL; ++i) {
-          const int r = wl + 32 * i;
-          const bool live = (RPL * 32 == P || r < P) && r < n;
+          const int r = t + PT * i;
+          const bool live = (RPL * PT == P || r < P) && r < n;
           ps[i] = live ? ps_s[r] : 0x7fffffff;
           const int sw = cta_swz(r);
 #pragma unroll
@@ -164,14 +188,14 @@ cta_exact_kernel(BatchView bv) {
 #pragma unroll 2
         for (; k < nb; ++k) {
           const int j = j0 + k;
-          // this lane's best candidate: larger |a| first, then smaller position;
+          // this thread's best candidate: larger |a| first, then smaller position;
           // eligible rows carry bit 63, NaN counts as zero (cblas idamax)
           unsigned long long kb = 0ull;
           unsigned pb = 0xffffffffu;
           double vb = 1.0;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
-            const int r = wl + 32 * i;
+            const int r = t + PT * i;
             if (r < n && ps[i] >= j) {
               const double v = fabs(pr[i][0]);
               const unsigned long long key =
@@ -179,33 +203,63 @@ cta_exact_kernel(BatchView bv) {
               if (key > kb || (key == kb && unsigned(ps[i]) < pb)) { kb = key; pb = unsigned(ps[i]); vb = pr[i][0]; }
             }
           }
-          // reciprocal of the lane's own candidate, overlapping the reduction
+          // reciprocal of the thread's own candidate, overlapping the reduction
           const double rb = __drcp_rn(vb);
           const unsigned hi = unsigned(kb >> 32), lo = unsigned(kb);
           const unsigned mh = __reduce_max_sync(FULL, hi);
           const unsigned ml = __reduce_max_sync(FULL, hi == mh ? lo : 0u);
-          const int ppos = int(__reduce_min_sync(FULL, (hi == mh && lo == ml) ? pb : 0xffffffffu));
+          int ppos = int(__reduce_min_sync(FULL, (hi == mh && lo == ml) ? pb : 0xffffffffu));
+          if (PW > 1) {
+            // best of the panel warps' candidates, same order
+            if (wl == 0) { cand[4 * wid] = mh; cand[4 * wid + 1] = ml; cand[4 * wid + 2] = unsigned(ppos); }
+            panel_bar(PT);
+            unsigned bh = cand[0], bl = cand[1], bp = cand[2];
+#pragma unroll
+            for (int w = 1; w < PW; ++w) {
+              const unsigned h2 = cand[4 * w], l2 = cand[4 * w + 1], p2 = cand[4 * w + 2];
+              if (h2 > bh || (h2 == bh && (l2 > bl || (l2 == bl && p2 < bp)))) { bh = h2; bl = l2; bp = p2; }
+            }
+            ppos = int(bp);
+          }
           apply_pending();
           int pi = 0;
           bool own = false;
 #pragma unroll
           for (int i = 0; i < RPL; ++i)
             if (ps[i] == ppos) { pi = i; own = true; }
-          const int pl = __ffs(__ballot_sync(FULL, own)) - 1;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
             if (ps[i] == ppos) ps[i] = j;
             else if (ps[i] == j) ps[i] = ppos;
           }
           double pv[B];
+          double rinv;
+          if (PW > 1) {
+            if (own) {
 #pragma unroll
-          for (int c = 0; c < B; ++c) {
-            double mine = pr[0][c];
+              for (int c = 0; c < B; ++c) {
+                double mine = pr[0][c];
 #pragma unroll
-            for (int i = 1; i < RPL; ++i) mine = (pi == i) ? pr[i][c] : mine;
-            pv[c] = __shfl_sync(FULL, mine, pl);
+                for (int i = 1; i < RPL; ++i) mine = (pi == i) ? pr[i][c] : mine;
+                pivbuf[c] = mine;
+              }
+              pivbuf[B] = rb;
+            }
+            panel_bar(PT);
+#pragma unroll
+            for (int c = 0; c < B; ++c) pv[c] = pivbuf[c];
+            rinv = pivbuf[B];
+          } else {
+            const int pl = __ffs(__ballot_sync(FULL, own)) - 1;
+#pragma unroll
+            for (int c = 0; c < B; ++c) {
+              double mine = pr[0][c];
+#pragma unroll
+              for (int i = 1; i < RPL; ++i) mine = (pi == i) ? pr[i][c] : mine;
+              pv[c] = __shfl_sync(FULL, mine, pl);
+            }
+            rinv = __shfl_sync(FULL, rb, pl);   // = fl(1/u_jj), correctly rounded
           }
-          const double rinv = __shfl_sync(FULL, rb, pl);   // = fl(1/u_jj), correctly rounded
           const double ujj = pv[0];
           if (__any_sync(FULL, ujj == 0.0)) { sing = true; break; }
           double lrow[RPL];
@@ -219,7 +273,7 @@ cta_exact_kernel(BatchView bv) {
           }
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
-            const int r = wl + 32 * i;
+            const int r = t + PT * i;
             const bool is_piv = (ps[i] == j);
             const bool below = ps[i] > j;
             const bool upd = r < n && !is_piv && (KIND == kInvert || below);
@@ -239,7 +293,7 @@ cta_exact_kernel(BatchView bv) {
           for (int c = 0; c < B; ++c) dpv[c] = pv[c];
           drinv = rinv;
           dk = k;
-          if (wl == 0) rinv_s[k] = rinv;
+          if (t == 0) rinv_s[k] = rinv;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
             const double first = pr[i][0];
@@ -250,7 +304,7 @@ cta_exact_kernel(BatchView bv) {
         }
         if (!sing) apply_pending();
         if (sing) {
-          if (wl == 0) flags[0] = 1;
+          if (t == 0) flags[0] = 1;
         } else {
 #pragma unroll 1
           for (; k < B; ++k) {
@@ -264,8 +318,8 @@ cta_exact_kernel(BatchView bv) {
           }
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
-            const int r = wl + 32 * i;
-            if ((RPL * 32 == P || r < P) && r < n) {
+            const int r = t + PT * i;
+            if ((RPL * PT == P || r < P) && r < n) {
               const int sw = cta_swz(r);
 #pragma unroll
               for (int c = 0; c < B; ++c) M[r * P + ((j0 + c) ^ sw)] = pr[i][c];
@@ -279,37 +333,34 @@ cta_exact_kernel(BatchView bv) {
       if (flags[0]) { singular = true; break; }
 
       // ---- 2. the panel's pivot rows at their own step, one thread per column
-      {
-        const int c = t % P;
-        const bool live = (t < P) && (c < j0 || c >= j0 + B) && (KIND == kInvert || c >= j0 + B);
-        if (live) {
-          int q[B];
-          double v[B];
+      for (int c = t; c < P; c += NT) {
+        if (!((c < j0 || c >= j0 + B) && (KIND == kInvert || c >= j0 + B))) continue;
+        int q[B];
+        double v[B];
 #pragma unroll
-          for (int k = 0; k < B; ++k) {
-            q[k] = (k < nb) ? perm[j0 + k] : 0;
-            v[k] = (k < nb) ? M[q[k] * P + (c ^ cta_swz(q[k]))] : 0.0;
-          }
+        for (int k = 0; k < B; ++k) {
+          q[k] = (k < nb) ? perm[j0 + k] : 0;
+          v[k] = (k < nb) ? M[q[k] * P + (c ^ cta_swz(q[k]))] : 0.0;
+        }
 #pragma unroll
-          for (int k = 1; k < B; ++k)
+        for (int k = 1; k < B; ++k)
 #pragma unroll
-            for (int k2 = 0; k2 < k; ++k2)
-              if (k < nb) v[k] = sub_rn(v[k], mul_rn(Mm[q[k] * MS + k2], v[k2]));
+          for (int k2 = 0; k2 < k; ++k2)
+            if (k < nb) v[k] = sub_rn(v[k], mul_rn(Mm[q[k] * MS + k2], v[k2]));
 #pragma unroll
-          for (int k = 0; k < B; ++k) Vs[k * P + c] = v[k];
+        for (int k = 0; k < B; ++k) Vs[k * P + c] = v[k];
 #pragma unroll
-          for (int k = 0; k < B; ++k) {
-            if (k < nb) {
-              double f = v[k];
-              if (KIND == kInvert) {
-                // scaled at its own step, then eliminated by the later pivots
-                f = mul_rn(f, rinv_s[k]);
+        for (int k = 0; k < B; ++k) {
+          if (k < nb) {
+            double f = v[k];
+            if (KIND == kInvert) {
+              // scaled at its own step, then eliminated by the later pivots
+              f = mul_rn(f, rinv_s[k]);
 #pragma unroll
-                for (int k2 = k + 1; k2 < B; ++k2)
-                  if (k2 < nb) f = fma(-Mm[q[k] * MS + k2], v[k2], f);
-              }
-              M[q[k] * P + (c ^ cta_swz(q[k]))] = f;
+              for (int k2 = k + 1; k2 < B; ++k2)
+                if (k2 < nb) f = fma(-Mm[q[k] * MS + k2], v[k2], f);
             }
+            M[q[k] * P + (c ^ cta_swz(q[k]))] = f;
           }
         }
       }
@@ -326,32 +377,37 @@ cta_exact_kernel(BatchView bv) {
           const int p = ps_s[row[u]];
           keep[u] = row[u] < n && (p < j0 || p >= j0 + nb) && (KIND == kInvert || p >= j0 + B);
         }
-        double a[RG][CB];
+#pragma unroll 1
+        for (int cg = 0; cg < CB; cg += CC) {
+          double a[RG][CC];
 #pragma unroll
-        for (int u = 0; u < RG; ++u) {
-          const int sw = cta_swz(row[u]);
-#pragma unroll
-          for (int c = 0; c < CB; ++c) a[u][c] = M[row[u] * P + ((tc + 8 * c) ^ sw)];
-        }
-#pragma unroll
-        for (int k = 0; k < B; ++k) {
-          double mk[RG], vk[CB];
-#pragma unroll
-          for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
-#pragma unroll
-          for (int c = 0; c < CB; ++c) vk[c] = Vs[k * P + tc + 8 * c];
-#pragma unroll
-          for (int u = 0; u < RG; ++u)
-#pragma unroll
-            for (int c = 0; c < CB; ++c) a[u][c] = sub_rn(a[u][c], mul_rn(mk[u], vk[c]));
-        }
-#pragma unroll
-        for (int u = 0; u < RG; ++u) {
-          if (keep[u]) {
+          for (int u = 0; u < RG; ++u) {
             const int sw = cta_swz(row[u]);
 #pragma unroll
-            for (int c = 0; c < CB; ++c)
-              if (c != jb && (KIND == kInvert || c > jb)) M[row[u] * P + ((tc + 8 * c) ^ sw)] = a[u][c];
+            for (int c = 0; c < CC; ++c) a[u][c] = M[row[u] * P + ((tc + 8 * (cg + c)) ^ sw)];
+          }
+#pragma unroll
+          for (int k = 0; k < B; ++k) {
+            double mk[RG], vk[CC];
+#pragma unroll
+            for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
+#pragma unroll
+            for (int c = 0; c < CC; ++c) vk[c] = Vs[k * P + tc + 8 * (cg + c)];
+#pragma unroll
+            for (int u = 0; u < RG; ++u)
+#pragma unroll
+              for (int c = 0; c < CC; ++c) a[u][c] = sub_rn(a[u][c], mul_rn(mk[u], vk[c]));
+          }
+#pragma unroll
+          for (int u = 0; u < RG; ++u) {
+            if (keep[u]) {
+              const int sw = cta_swz(row[u]);
+#pragma unroll
+              for (int c = 0; c < CC; ++c) {
+                const int cb = cg + c;
+                if (cb != jb && (KIND == kInvert || cb > jb)) M[row[u] * P + ((tc + 8 * cb) ^ sw)] = a[u][c];
+              }
+            }
           }
         }
       }
@@ -369,15 +425,13 @@ cta_exact_kernel(BatchView bv) {
 
     if (KIND == kInvert) {
       // A^-1[q][c] = W[q][ps[c]] with W the physically permuted array, i.e.
-      // row perm[q] of the in-place result (A^-1 = W P, P from GSL's permutation)
+      // row perm[q] of the in-place result (A^-1 = W P, P from GSL's permutation);
+      // a warp per output row
       double* __restrict__ Og = bv.out + bv.offA[s];
-      const int c = t % P;
-      if (c < n) {
-        const int pc = ps_s[c];
-        for (int q = t / P; q < n; q += NT / P) {
-          const int r = perm[q];
-          Og[int64_t(q) * n + c] = M[r * P + (pc ^ cta_swz(r))];
-        }
+      for (int q = wid; q < n; q += NW) {
+        const int r = perm[q], sw = cta_swz(r);
+        double* __restrict__ orow = Og + int64_t(q) * n;
+        for (int c = wl; c < n; c += 32) orow[c] = M[r * P + (ps_s[c] ^ sw)];
       }
       if (t == 0) {
         bv.status[s] = kOk;
@@ -386,8 +440,8 @@ cta_exact_kernel(BatchView bv) {
     } else {
       // LU_svx (lu.c:324-360): permute b, unit-lower then upper sweep, each entry
       // in GSL's order; row q of the factors is row perm[q] of M
-      double* vec = Vs;                    // [P] (Vs holds B*P >= 2P doubles)
-      double* xs = Vs + P;
+      double* vec = Vs;                    // [P]
+      double* xs = Vs + P;                 // [P]
       if (wid == 0) {
         const int64_t ov = bv.offv[s];
         for (int i = wl; i < n; i += 32) vec[i] = bv.b[ov + perm[i]];

@@ -1,4 +1,4 @@
-// CTA-per-system kernels for n > 160 (large macro atoms, full ion matrices).
+// CTA-per-system kernels for n > 256 (large macro atoms, full ion matrices).
 //
 // The system is factorised in a global-memory workspace W (the output buffer
 // for an inverse, a per-CTA scratch slab for a solve; a few hundred systems
