@@ -63,8 +63,8 @@ struct KernelSpec {
 
 // size classes of the small family (padded row length NP, lanes per system G)
 static const int kSmallNP[] = {4, 8, 12, 16, 20, 24, 28, 32};
-static const int kCtaP[] = {48, 64, 96, 128, 160, 192, 224, 256};
-constexpr int kCtaClasses = 8;
+static const int kCtaP[] = {48, 64, 96, 128, 160, 192, 208, 224, 256};
+constexpr int kCtaClasses = 9;
 
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
@@ -115,17 +115,20 @@ static KernelSpec cta_spec(int cls) {
     k.work_slab = Sh::slab;                                                             \
     break;                                                                              \
   }
-  // order classes up to 160 keep the matrix in shared memory; above, in a
-  // global workspace slab per CTA with two panel warps
+  // order classes up to 64 keep the matrix in shared memory; above, in a
+  // global workspace slab per CTA, where more CTAs per SM (more pivot chains in
+  // flight) beat the faster memory: measured on B200, n = 90 / 120 / 150
+  // inverses ran 1.1x / 1.6x / 1.3x faster from L2 than from shared memory
   switch (cls) {
     SS_CTA(0, 48, 96, 2, 6, 1, false, 0)
     SS_CTA(1, 64, 128, 2, 8, 1, false, 0)
-    SS_CTA(2, 96, 192, 2, 12, 1, false, 0)
-    SS_CTA(3, 128, 256, 2, 16, 1, false, 0)
-    SS_CTA(4, 160, 320, 2, 20, 1, false, 0)
+    SS_CTA(2, 96, 128, 2, 6, 2, true, 4)
+    SS_CTA(3, 128, 128, 2, 8, 2, true, 4)
+    SS_CTA(4, 160, 160, 2, 10, 3, true, 3)
     SS_CTA(5, 192, 256, 2, 8, 3, true, 2)
-    SS_CTA(6, 224, 224, 2, 7, 4, true, 2)
-    SS_CTA(7, 256, 256, 2, 8, 4, true, 2)
+    SS_CTA(6, 208, 416, 2, 13, 4, true, 1)
+    SS_CTA(7, 224, 224, 2, 7, 4, true, 2)
+    SS_CTA(8, 256, 256, 2, 8, 4, true, 2)
     default: break;
   }
 #undef SS_CTA

@@ -4,8 +4,8 @@
 // The padded P x P matrix is held row-major with its columns XOR-swizzled
 // inside 16-column groups (row, column and tile accesses are then free of
 // shared-memory bank conflicts and stay inside one 128-byte line): in shared
-// memory for P <= 160, in an L2-resident global workspace slab per CTA above
-// that, where several CTAs per SM keep several pivot chains in flight.  Rows
+// memory for the smallest classes, in an L2-resident global workspace slab per
+// CTA above them, where several CTAs per SM keep several pivot chains in flight.  Rows
 // never move: each physical row carries its current position (ps), and
 // perm[q] names the row at position q, so GSL's row swaps cost two integer
 // stores and ties in the pivot search break on positions exactly as GSL's
