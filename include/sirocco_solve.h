@@ -110,6 +110,32 @@ int sirocco_plan_destroy(sirocco_plan *plan);
 /* Text of the last library error on this thread. */
 const char *sirocco_last_error(void);
 
+/* Macro-atom jumping matrices of a whole cycle (the reference's
+   calc_matom_matrix, source/macro_accelerate.c:311-334, called per cell from
+   calc_all_matom_matrices :1054-1061).  For every cell s, N_s = I - Q/Q_norm
+   (n[s] x n[s], row-major at offA[s]) is inverted GSL-exactly and
+   B_s = N_s^-1 diag(R_s) is written at offA[s] of B, with R_s the n[s] diagonal
+   entries of R at offv[s].  C, which may be null, receives the row running
+   totals of B (C[r][c] = B[r][0] + ... + B[r][c], summed left to right as
+   matom_deactivation_from_matrix, :995-1008, sums them), so that a draw is a
+   search of one row of C.  status[s] is invert_matrix's code; a singular cell
+   gets B = C = 0, as the reference's zero-filled inverse buffer gives.  Layout
+   arrays are host arrays; N, R, B, C and status are all host or all device
+   pointers (device: B and C can stay resident for matom_sample_batched). */
+int matom_matrices_batched(int nsys, const int *n, const int64_t *offA, const int64_t *offv, const double *N,
+                           const double *R, double *B, double *C, int *status);
+
+/* Batched draws of the macro-atom deactivation (matom_deactivation_from_matrix,
+   source/macro_accelerate.c:951-1018) from the running totals C of
+   matom_matrices_batched: query i activates level level[i] of cell sys[i] with
+   the uniform number z[i] and gets target[i] = 0 if z <= 0, else the first
+   column whose running total is not below z; -1 if the row total stays below z
+   (where the reference's loop would read past the row), -2 for a cell or level
+   out of range.  n and offA are the host layout arrays of C; C, sys, level, z
+   and target are all host or all device pointers. */
+int matom_sample_batched(int nq, int nsys, const int *n, const int64_t *offA, const double *C, const int *sys,
+                         const int *level, const double *z, int *target);
+
 /* No counterpart in the reference.  Batched solve that allocates no memory at
    all, for callers that cannot let a library allocate on the GPU: host codes
    that reserve the device's memory up front for their own arena (a cudaMalloc

@@ -23,6 +23,7 @@
 #include "../../include/sirocco_solve.h"
 #include "kernels_cta.cuh"
 #include "kernels_global.cuh"
+#include "kernels_matom.cuh"
 #include "kernels_mixed.cuh"
 #include "kernels_small.cuh"
 
@@ -425,6 +426,7 @@ struct Context {
   std::unordered_map<uint64_t, std::unique_ptr<Pipeline>> pipes;
   std::vector<uint64_t> pipe_order;
   DevBuf bA, bb, bx, bst;
+  DevBuf bR, bC, bOv, bN, bOa, bQs, bQl, bQz, bQt;   // macro-atom epilogue and draws
   int mode = SIROCCO_FP64;
   ~Context() { release(); }
   void release() {
@@ -633,6 +635,112 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
   return 0;
 }
 
+// ------------------------------------------------------------ macro atoms --
+// B = N^-1 diag(R) per cell and the row running totals of B, after the
+// GSL-exact FP64 inverse (the reference's calc_matom_matrix,
+// source/macro_accelerate.c:311-334, and the walk of
+// matom_deactivation_from_matrix, :995-1008).
+static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t* offv, const double* N,
+                     const double* R, double* B, double* C, int* status) {
+  if (nsys == 0) return 0;
+  if (nsys < 0 || !n || !offA || !offv || !N || !R || !B || !status) {
+    set_error("invalid macro-atom arguments");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  sirocco_plan* p = nullptr;
+  rc = c->get_plan(kInvert, nsys, n, offA, nullptr, SIROCCO_FP64, &p);
+  if (rc) return rc;
+  int64_t totV = 0;
+  for (int s = 0; s < nsys; ++s) totV = std::max<int64_t>(totV, offv[s] + n[s]);
+  if ((rc = c->bOv.ensure(sizeof(int64_t) * size_t(nsys)))) return rc;
+  int64_t* dOv = static_cast<int64_t*>(c->bOv.ptr);
+  SS_CUDA(cudaMemcpyAsync(dOv, offv, sizeof(int64_t) * size_t(nsys), cudaMemcpyHostToDevice, c->stream));
+  const int grid = std::max(1, std::min(nsys, p->num_sms * 16));
+  if (is_device_ptr(N)) {
+    rc = plan_run(p, N, nullptr, B, status, nullptr, c->stream);
+    if (rc) return rc;
+    matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA, dOv, B, R, C, status);
+    SS_CUDA(cudaGetLastError());
+    SS_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+  }
+  const size_t bytesA = sizeof(double) * size_t(p->totA), bytesV = sizeof(double) * size_t(totV);
+  if ((rc = c->bA.ensure(bytesA)) || (rc = c->bx.ensure(bytesA)) || (rc = c->bR.ensure(bytesV)) ||
+      (rc = c->bst.ensure(sizeof(int) * size_t(nsys))) || (C && (rc = c->bC.ensure(bytesA))))
+    return rc;
+  double* dN = static_cast<double*>(c->bA.ptr);
+  double* dB = static_cast<double*>(c->bx.ptr);
+  double* dR = static_cast<double*>(c->bR.ptr);
+  double* dC = C ? static_cast<double*>(c->bC.ptr) : nullptr;
+  int* dst = static_cast<int*>(c->bst.ptr);
+  SS_CUDA(cudaMemcpyAsync(dN, N, bytesA, cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(dR, R, bytesV, cudaMemcpyHostToDevice, c->stream));
+  rc = plan_run(p, dN, nullptr, dB, dst, nullptr, c->stream);
+  if (rc) return rc;
+  matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA, dOv, dB, dR, dC, dst);
+  SS_CUDA(cudaGetLastError());
+  SS_CUDA(cudaMemcpyAsync(B, dB, bytesA, cudaMemcpyDeviceToHost, c->stream));
+  if (C) SS_CUDA(cudaMemcpyAsync(C, dC, bytesA, cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaMemcpyAsync(status, dst, sizeof(int) * size_t(nsys), cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+static int run_matom_sample(int nq, int nsys, const int* n, const int64_t* offA, const double* C, const int* sys,
+                            const int* level, const double* z, int* target) {
+  if (nq == 0) return 0;
+  if (nq < 0 || nsys < 1 || !n || !offA || !C || !sys || !level || !z || !target) {
+    set_error("invalid macro-atom draw arguments");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  int64_t totA = 0;
+  for (int s = 0; s < nsys; ++s) {
+    if (n[s] < 1) {
+      set_error("system %d has order %d", s, n[s]);
+      return SIROCCO_EINVAL;
+    }
+    totA = std::max<int64_t>(totA, offA[s] + int64_t(n[s]) * n[s]);
+  }
+  if ((rc = c->bN.ensure(sizeof(int) * size_t(nsys))) || (rc = c->bOa.ensure(sizeof(int64_t) * size_t(nsys))))
+    return rc;
+  int* dn = static_cast<int*>(c->bN.ptr);
+  int64_t* doa = static_cast<int64_t*>(c->bOa.ptr);
+  SS_CUDA(cudaMemcpyAsync(dn, n, sizeof(int) * size_t(nsys), cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(doa, offA, sizeof(int64_t) * size_t(nsys), cudaMemcpyHostToDevice, c->stream));
+  const int grid = (nq + 255) / 256;
+  if (is_device_ptr(C)) {
+    matom_sample_kernel<<<grid, 256, 0, c->stream>>>(nq, nsys, dn, doa, C, sys, level, z, target);
+    SS_CUDA(cudaGetLastError());
+    SS_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+  }
+  const size_t bytesC = sizeof(double) * size_t(totA);
+  if ((rc = c->bC.ensure(bytesC)) || (rc = c->bQs.ensure(sizeof(int) * size_t(nq))) ||
+      (rc = c->bQl.ensure(sizeof(int) * size_t(nq))) || (rc = c->bQz.ensure(sizeof(double) * size_t(nq))) ||
+      (rc = c->bQt.ensure(sizeof(int) * size_t(nq))))
+    return rc;
+  double* dC = static_cast<double*>(c->bC.ptr);
+  int* ds = static_cast<int*>(c->bQs.ptr);
+  int* dl = static_cast<int*>(c->bQl.ptr);
+  double* dz = static_cast<double*>(c->bQz.ptr);
+  int* dt = static_cast<int*>(c->bQt.ptr);
+  SS_CUDA(cudaMemcpyAsync(dC, C, bytesC, cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(ds, sys, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(dl, level, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(dz, z, sizeof(double) * size_t(nq), cudaMemcpyHostToDevice, c->stream));
+  matom_sample_kernel<<<grid, 256, 0, c->stream>>>(nq, nsys, dn, doa, dC, ds, dl, dz, dt);
+  SS_CUDA(cudaGetLastError());
+  SS_CUDA(cudaMemcpyAsync(target, dt, sizeof(int) * size_t(nq), cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
 // single system through the host path, honouring the reference's "output
 // untouched on a singular matrix" behaviour
 static int run_single(int kind, double* A, const double* b, int size, double* out, int* code) {
@@ -820,6 +928,16 @@ int sirocco_plan_destroy(sirocco_plan* plan) {
 }
 
 const char* sirocco_last_error(void) { return g_last_error.c_str(); }
+
+int matom_matrices_batched(int nsys, const int* n, const int64_t* offA, const int64_t* offv, const double* N,
+                           const double* R, double* B, double* C, int* status) {
+  return ss::run_matom(nsys, n, offA, offv, N, R, B, C, status);
+}
+
+int matom_sample_batched(int nq, int nsys, const int* n, const int64_t* offA, const double* C, const int* sys,
+                         const int* level, const double* z, int* target) {
+  return ss::run_matom_sample(nq, nsys, n, offA, C, sys, level, z, target);
+}
 
 int solve_matrix_batched_noalloc(int nsys, int nmax, const int* n, const int64_t* offA, const double* A,
                                  const int64_t* offv, const double* b, double* x, int* status, void* stream) {

@@ -29,6 +29,7 @@ EXPORTS = (
     "solve_matrix_batched", "invert_matrix_batched", "sirocco_set_precision",
     "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
     "sirocco_plan_destroy", "sirocco_last_error", "solve_matrix_batched_noalloc",
+    "matom_matrices_batched", "matom_sample_batched",
 )
 
 _lib = None
@@ -77,6 +78,10 @@ def load() -> ctypes.CDLL:
     lib.sirocco_last_error.restype = c_char_p
     lib.solve_matrix_batched_noalloc.argtypes = [c_int, c_int] + [c_void_p] * 8
     lib.solve_matrix_batched_noalloc.restype = c_int
+    lib.matom_matrices_batched.argtypes = [c_int] + [c_void_p] * 8
+    lib.matom_matrices_batched.restype = c_int
+    lib.matom_sample_batched.argtypes = [c_int, c_int] + [c_void_p] * 7
+    lib.matom_sample_batched.restype = c_int
     _lib = lib
     return lib
 
@@ -156,6 +161,39 @@ def invert_batched(batch: Batch, mode: int = FP64, out: np.ndarray | None = None
     rc = lib.invert_matrix_batched(batch.nsys, _ptr(n), _ptr(batch.offA), _ptr(batch.A), _ptr(out), _ptr(st))
     _check(rc, "invert_matrix_batched")
     return out, st
+
+
+def matom_matrices(batch: Batch, R: np.ndarray, offv: np.ndarray, cumulative: bool = True):
+    """B = N^-1 diag(R) per cell and its row running totals through
+    matom_matrices_batched; returns (B, C or None, status)."""
+    lib = load()
+    n = np.ascontiguousarray(batch.n, np.int32)
+    offv = np.ascontiguousarray(offv, np.int64)
+    R = np.ascontiguousarray(R, np.float64)
+    B = np.full(batch.A.size, np.nan)
+    C = np.full(batch.A.size, np.nan) if cumulative else None
+    st = np.full(batch.nsys, -99, np.int32)
+    rc = lib.matom_matrices_batched(batch.nsys, _ptr(n), _ptr(batch.offA), _ptr(offv), _ptr(batch.A), _ptr(R),
+                                    _ptr(B), _ptr(C) if C is not None else None, _ptr(st))
+    _check(rc, "matom_matrices_batched")
+    return B, C, st
+
+
+def matom_sample(n: np.ndarray, offA: np.ndarray, C: np.ndarray, sys: np.ndarray, level: np.ndarray,
+                 z: np.ndarray) -> np.ndarray:
+    """Deactivation targets of a batch of draws through matom_sample_batched."""
+    lib = load()
+    n = np.ascontiguousarray(n, np.int32)
+    offA = np.ascontiguousarray(offA, np.int64)
+    sys = np.ascontiguousarray(sys, np.int32)
+    level = np.ascontiguousarray(level, np.int32)
+    z = np.ascontiguousarray(z, np.float64)
+    C = np.ascontiguousarray(C, np.float64)
+    target = np.full(sys.size, -99, np.int32)
+    rc = lib.matom_sample_batched(sys.size, n.size, _ptr(n), _ptr(offA), _ptr(C), _ptr(sys), _ptr(level), _ptr(z),
+                                  _ptr(target))
+    _check(rc, "matom_sample_batched")
+    return target
 
 
 class Plan:

@@ -115,6 +115,18 @@ def macro_matrix(rng, n: int, density=0.25, qrange=(1e-8, 1.0),
     return np.eye(n) - q
 
 
+def matom_cells(sizes, seed, density=0.25):
+    """Macro-atom cells for the B = N^-1 diag(R) epilogue: N = I - Q/Q_norm from
+    the config-1 generator and R the normalised deactivation rate of each level,
+    so that R_u - sum_t N_ut = 0 (the normalisation calc_matom_matrix checks,
+    source/macro_accelerate.c:288-300).  Returns (invert batch of N, R, offv)."""
+    rng = np.random.default_rng(seed)
+    mats = [macro_matrix(rng, int(n), density=density) for n in sizes]
+    R = np.concatenate([m.sum(axis=1) for m in mats]) if mats else np.zeros(0)
+    b = _pack("invert", mats)
+    return b, R, offsets(np.asarray(b.n), False)
+
+
 def _pack(kind, mats, rhs=None) -> Batch:
     n = np.array([m.shape[0] for m in mats], np.int32)
     offA = offsets(n, True)
