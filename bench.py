@@ -51,7 +51,7 @@ HBM_FALLBACK_GBS = 6650.0
 TRAFFIC = {
     1: ("cta64", 438.2 / 487.7, "profiles/cta_exact_kernel_inverse_8192x61.md"),
     0: ("small28", 25.0 / 25.66, "profiles/small_exact_kernel_solve_4096x27.md"),
-    3: ("global", 623.7 / 336.0, "profiles/global_exact_kernel_inverse_n129-200.md"),
+    3: ("cta192", 2294.0 / 248.6, "profiles/cta_exact_kernel_inverse_n161-192_workspace.md"),
 }
 
 WORKLOADS = {
