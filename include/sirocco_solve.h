@@ -110,6 +110,33 @@ int sirocco_plan_destroy(sirocco_plan *plan);
 /* Text of the last library error on this thread. */
 const char *sirocco_last_error(void);
 
+/* Lock-step ionisation balance: the n_e iteration of matrix_ion_populations
+   (source/matrix_ion.c:219-382) for ncell cells at once, one batched solve per
+   round over every unfinished cell.  Ions 0..nions-1 form nelem elements;
+   element e holds ions elem_first[e] .. elem_first[e]+elem_n[e]-1 and istate[]
+   is each ion's charge + 1 (ion[].istate).  h_elem is hydrogen's element (-1:
+   none).  elem_dens[c*nelem + e] is the element number density of cell c.
+   ne[c] (in: the starting n_e, out: the converged one) and den[c*nions + i]
+   (in: starting ion fractions of each element, out: converged ones) are
+   updated only for cells that converge.  Each round the library calls
+   `assemble` for the cells still iterating: for cell cells[i] at n_e ne[i] and
+   neutral / ionised hydrogen densities nh1[i], nh2[i] it fills the rate matrix
+   (populate_ion_rate_matrix, matrix_ion.c:445-659) as one row-major block per
+   element, cell after cell (A) and the matching right-hand sides (b, nions per
+   cell); a nonzero return aborts with SIROCCO_EINVAL.  After each solve the
+   cell follows the reference: populations floored at DENSITY_MIN (1e-20), new
+   n_e from the ion charges, converged when |n_e - n_e'| / n_e' < 0.03 or
+   n_e' < 1e-6, otherwise n_e <- (n_e + n_e') / 2, at most 200 rounds.
+   status[c]: 0 converged, -1 a singular block (solve_matrix code 4, the
+   reference's return -1), -2 no convergence in 200 rounds.  iters[c]: rounds
+   used.  The solves use the precision mode of sirocco_set_precision.  All
+   arrays are host arrays. */
+typedef int (*sirocco_ion_assemble_fn)(void *user, int ncell, const int *cells, const double *ne, const double *nh1,
+                                       const double *nh2, double *A, double *b);
+int ion_populations_lockstep(int ncell, int nions, int nelem, const int *elem_first, const int *elem_n,
+                             const int *istate, int h_elem, const double *elem_dens, double *ne, double *den,
+                             sirocco_ion_assemble_fn assemble, void *user, int *status, int *iters);
+
 /* Macro-atom jumping matrices of a whole cycle (the reference's
    calc_matom_matrix, source/macro_accelerate.c:311-334, called per cell from
    calc_all_matom_matrices :1054-1061).  For every cell s, N_s = I - Q/Q_norm

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
@@ -190,6 +191,8 @@ struct sirocco_plan {
   int64_t* d_offv = nullptr;
   int* d_list = nullptr;
   double* d_scratch = nullptr;
+  int64_t scratch_elems = 0;   // workspace doubles the buckets need
+  bool own_scratch = true;     // false: d_scratch points into a pipeline's shared workspace
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
   cudaEvent_t ev_fork = nullptr;
@@ -203,7 +206,7 @@ static void plan_free(sirocco_plan* p) {
   cudaFree(p->d_offA);
   cudaFree(p->d_offv);
   cudaFree(p->d_list);
-  cudaFree(p->d_scratch);
+  if (p->own_scratch) cudaFree(p->d_scratch);
   for (auto s : p->side) cudaStreamDestroy(s);
   for (auto e : p->ev) cudaEventDestroy(e);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
@@ -211,7 +214,7 @@ static void plan_free(sirocco_plan* p) {
 }
 
 static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, const int64_t* offA,
-                      const int64_t* offv, int mode) {
+                      const int64_t* offv, int mode, bool alloc_scratch = true) {
   *out = nullptr;
   if (nsys < 0 || (nsys > 0 && (!n || !offA || (kind == kSolve && !offv)))) {
     set_error("invalid plan arguments");
@@ -300,7 +303,9 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
       SS_CUDA(cudaMemcpy(p->d_offv, offv, sizeof(int64_t) * nsys, cudaMemcpyHostToDevice));
     }
   }
-  if (scratch_elems > 0) SS_CUDA(cudaMalloc(&p->d_scratch, sizeof(double) * scratch_elems));
+  p->scratch_elems = scratch_elems;
+  p->own_scratch = alloc_scratch;
+  if (alloc_scratch && scratch_elems > 0) SS_CUDA(cudaMalloc(&p->d_scratch, sizeof(double) * scratch_elems));
   // one side stream per bucket beyond the first
   for (size_t i = 1; i < p->buckets.size(); ++i) {
     cudaStream_t st;
@@ -408,8 +413,12 @@ struct Pipeline {
     sirocco_plan* plan;
   };
   std::vector<Chunk> chunks;
+  // chunk k runs on pipeline stream k % kPipeStreams, after the chunks before it
+  // on that stream: one workspace per stream serves all of that stream's chunks
+  double* scratch = nullptr;
   ~Pipeline() {
     for (auto& c : chunks) plan_free(c.plan);
+    cudaFree(scratch);
   }
 };
 
@@ -492,10 +501,20 @@ struct Context {
         rv[s - s0] = offv ? offv[s] - c.v0 : 0;
       }
       c.plan = nullptr;
-      int rc = plan_build(&c.plan, kind, s1 - s0, n + s0, ra.data(), offv ? rv.data() : nullptr, md);
-      if (rc) return rc;
+      int rc = plan_build(&c.plan, kind, s1 - s0, n + s0, ra.data(), offv ? rv.data() : nullptr, md, false);
+      if (rc) {
+        plan_free(c.plan);
+        return rc;
+      }
       pl->chunks.push_back(c);
       s0 = s1;
+    }
+    int64_t per_stream = 0;
+    for (auto& c : pl->chunks) per_stream = std::max(per_stream, c.plan->scratch_elems);
+    if (per_stream > 0) {
+      SS_CUDA(cudaMalloc(&pl->scratch, sizeof(double) * per_stream * kPipeStreams));
+      for (size_t k = 0; k < pl->chunks.size(); ++k)
+        pl->chunks[k].plan->d_scratch = pl->scratch + per_stream * int64_t(k % kPipeStreams);
     }
     if (pipe_order.size() >= 8) {
       pipes.erase(pipe_order.front());
@@ -741,6 +760,134 @@ static int run_matom_sample(int nq, int nsys, const int* n, const int64_t* offA,
   return 0;
 }
 
+// ------------------------------------------------------- ion populations --
+// Lock-step n_e iteration over many cells: the loop of matrix_ion_populations
+// (source/matrix_ion.c:219-382) run for every cell at once, one batched solve
+// per round over the per-element blocks of all cells that have not finished.
+// The reference's rate matrix is block-diagonal by element (its first row of
+// each element's block is the conservation row), so LU with partial pivoting on
+// the full matrix only ever meets exact zeros outside a block: the per-element
+// solves give the full matrix's solution and codes bit for bit.
+constexpr double kDensityMin = 1.0e-20;   // atomic.h:9
+constexpr double kFracError = 0.03;       // python.h:1212
+constexpr int kMaxIterations = 200;       // python.h:1211
+
+static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_first, const int* elem_n,
+                            const int* istate, int h_elem, const double* elem_dens, double* ne, double* den,
+                            sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
+  if (ncell == 0) return 0;
+  if (ncell < 0 || nions < 1 || nelem < 1 || !elem_first || !elem_n || !istate || !elem_dens || !ne || !den ||
+      !assemble || !status || !iters || h_elem >= nelem) {
+    set_error("invalid lock-step arguments");
+    return SIROCCO_EINVAL;
+  }
+  std::vector<int> elem_of(nions, -1);
+  int64_t blkA = 0;
+  for (int e = 0; e < nelem; ++e) {
+    if (elem_n[e] < 1 || elem_first[e] < 0 || elem_first[e] + elem_n[e] > nions) {
+      set_error("element %d: ions [%d, %d) outside 0..%d", e, elem_first[e], elem_first[e] + elem_n[e], nions);
+      return SIROCCO_EINVAL;
+    }
+    for (int k = 0; k < elem_n[e]; ++k) {
+      if (elem_of[elem_first[e] + k] >= 0) {
+        set_error("ion %d belongs to two elements", elem_first[e] + k);
+        return SIROCCO_EINVAL;
+      }
+      elem_of[elem_first[e] + k] = e;
+    }
+    blkA += int64_t(elem_n[e]) * elem_n[e];
+  }
+  for (int i = 0; i < nions; ++i)
+    if (elem_of[i] < 0) {
+      set_error("ion %d belongs to no element", i);
+      return SIROCCO_EINVAL;
+    }
+  std::vector<double> xne(ne, ne + ncell), cur(den, den + size_t(ncell) * nions);
+  std::vector<int> active(ncell);
+  for (int c = 0; c < ncell; ++c) {
+    active[c] = c;
+    status[c] = -2;
+    iters[c] = 0;
+  }
+  std::vector<double> A, b, x, nh1, nh2, nea;
+  std::vector<int> n, st;
+  std::vector<int64_t> offA, offv;
+  for (int it = 0; it < kMaxIterations && !active.empty(); ++it) {
+    const int na = int(active.size());
+    nea.resize(na);
+    nh1.assign(na, 0.0);
+    nh2.assign(na, 0.0);
+    for (int i = 0; i < na; ++i) {
+      const int c = active[i];
+      nea[i] = xne[c];
+      if (h_elem >= 0) {
+        // neutral and ionised hydrogen densities for charge exchange (matrix_ion.c:228-238)
+        const double* cd = &cur[size_t(c) * nions];
+        const double dh = elem_dens[size_t(c) * nelem + h_elem];
+        for (int k = 0; k < elem_n[h_elem]; ++k) {
+          const int nn = elem_first[h_elem] + k;
+          if (istate[nn] == 1) nh1[i] = cd[nn] * dh;
+          if (istate[nn] == 2) nh2[i] = cd[nn] * dh;
+        }
+      }
+    }
+    A.assign(size_t(na) * blkA, 0.0);
+    b.assign(size_t(na) * nions, 0.0);
+    const int arc = assemble(user, na, active.data(), nea.data(), nh1.data(), nh2.data(), A.data(), b.data());
+    if (arc != 0) {
+      set_error("assembly callback returned %d", arc);
+      return SIROCCO_EINVAL;
+    }
+    const int nsys = na * nelem;
+    n.resize(nsys);
+    offA.resize(nsys);
+    offv.resize(nsys);
+    st.assign(nsys, 0);
+    x.assign(size_t(na) * nions, 0.0);
+    for (int i = 0, s = 0; i < na; ++i) {
+      int64_t oa = int64_t(i) * blkA;
+      for (int e = 0; e < nelem; ++e, ++s) {
+        n[s] = elem_n[e];
+        offA[s] = oa;
+        offv[s] = int64_t(i) * nions + elem_first[e];
+        oa += int64_t(elem_n[e]) * elem_n[e];
+      }
+    }
+    int rc = run_batched(kSolve, nsys, n.data(), offA.data(), A.data(), offv.data(), b.data(), x.data(), st.data(),
+                         ctx()->mode);
+    if (rc) return rc;
+    std::vector<int> next;
+    for (int i = 0; i < na; ++i) {
+      const int c = active[i];
+      bool singular = false;
+      for (int e = 0; e < nelem; ++e) singular |= st[size_t(i) * nelem + e] == kSolveSingular;
+      iters[c] = it + 1;
+      if (singular) {   // matrix_ion.c:295-299: the cell keeps its old populations
+        status[c] = -1;
+        continue;
+      }
+      double* nd = &cur[size_t(c) * nions];
+      const double* xi = &x[size_t(i) * nions];
+      for (int nn = 0; nn < nions; ++nn) nd[nn] = xi[nn] < kDensityMin ? kDensityMin : xi[nn];
+      double xnew = 0.0;
+      for (int nn = 0; nn < nions; ++nn)
+        xnew += nd[nn] * (istate[nn] - 1) * elem_dens[size_t(c) * nelem + elem_of[nn]];
+      if (xnew < kDensityMin) xnew = kDensityMin;
+      if (std::fabs((xne[c] - xnew) / xnew) < kFracError || xnew < 1.e-6) {
+        status[c] = 0;
+        ne[c] = xnew;
+        std::copy(nd, nd + nions, den + size_t(c) * nions);
+        continue;
+      }
+      xne[c] = (xnew + xne[c]) / 2.;
+      next.push_back(c);
+    }
+    active.swap(next);
+  }
+  // cells still active ran out of iterations (matrix_ion.c:366-382): status -2, inputs kept
+  return 0;
+}
+
 // single system through the host path, honouring the reference's "output
 // untouched on a singular matrix" behaviour
 static int run_single(int kind, double* A, const double* b, int size, double* out, int* code) {
@@ -937,6 +1084,13 @@ int matom_matrices_batched(int nsys, const int* n, const int64_t* offA, const in
 int matom_sample_batched(int nq, int nsys, const int* n, const int64_t* offA, const double* C, const int* sys,
                          const int* level, const double* z, int* target) {
   return ss::run_matom_sample(nq, nsys, n, offA, C, sys, level, z, target);
+}
+
+int ion_populations_lockstep(int ncell, int nions, int nelem, const int* elem_first, const int* elem_n,
+                             const int* istate, int h_elem, const double* elem_dens, double* ne, double* den,
+                             sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
+  return ss::run_ion_lockstep(ncell, nions, nelem, elem_first, elem_n, istate, h_elem, elem_dens, ne, den, assemble,
+                              user, status, iters);
 }
 
 int solve_matrix_batched_noalloc(int nsys, int nmax, const int* n, const int64_t* offA, const double* A,

@@ -29,10 +29,14 @@ EXPORTS = (
     "solve_matrix_batched", "invert_matrix_batched", "sirocco_set_precision",
     "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
     "sirocco_plan_destroy", "sirocco_last_error", "solve_matrix_batched_noalloc",
-    "matom_matrices_batched", "matom_sample_batched",
+    "matom_matrices_batched", "matom_sample_batched", "ion_populations_lockstep",
 )
 
 _lib = None
+
+# assembly callback of ion_populations_lockstep
+ASSEMBLE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_double),
+                               POINTER(c_double), POINTER(c_double), POINTER(c_double))
 
 
 class EngineError(RuntimeError):
@@ -82,6 +86,9 @@ def load() -> ctypes.CDLL:
     lib.matom_matrices_batched.restype = c_int
     lib.matom_sample_batched.argtypes = [c_int, c_int] + [c_void_p] * 7
     lib.matom_sample_batched.restype = c_int
+    lib.ion_populations_lockstep.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                                             c_void_p, c_void_p, ASSEMBLE_FN, c_void_p, c_void_p, c_void_p]
+    lib.ion_populations_lockstep.restype = c_int
     _lib = lib
     return lib
 
@@ -194,6 +201,44 @@ def matom_sample(n: np.ndarray, offA: np.ndarray, C: np.ndarray, sys: np.ndarray
                                   _ptr(target))
     _check(rc, "matom_sample_batched")
     return target
+
+
+def ion_populations_lockstep(elem_first, elem_n, istate, h_elem: int, elem_dens: np.ndarray, ne: np.ndarray,
+                             den: np.ndarray, assemble):
+    """The n_e iteration of every cell at once (ion_populations_lockstep).
+
+    ``assemble(cells, ne, nh1, nh2, A, b)`` fills, in place, the per-element
+    rate-matrix blocks of the listed cells (A, packed cell after cell, each
+    block row-major) and their right-hand sides (b, nions per cell).
+    ``ne`` [ncell] and ``den`` [ncell, nions] are updated in place for the cells
+    that converge; returns (status, iters).
+    """
+    import traceback
+    lib = load()
+    elem_first = np.ascontiguousarray(elem_first, np.int32)
+    elem_n = np.ascontiguousarray(elem_n, np.int32)
+    istate = np.ascontiguousarray(istate, np.int32)
+    elem_dens = np.ascontiguousarray(elem_dens, np.float64)
+    assert ne.dtype == np.float64 and ne.flags.c_contiguous and den.dtype == np.float64 and den.flags.c_contiguous
+    ncell, nions = den.shape
+    blk = int((elem_n.astype(np.int64) ** 2).sum())
+
+    def cb(user, n, cells, ne_p, nh1_p, nh2_p, a_p, b_p):
+        try:
+            assemble(np.ctypeslib.as_array(cells, (n,)).copy(), np.ctypeslib.as_array(ne_p, (n,)).copy(),
+                     np.ctypeslib.as_array(nh1_p, (n,)).copy(), np.ctypeslib.as_array(nh2_p, (n,)).copy(),
+                     np.ctypeslib.as_array(a_p, (n * blk,)), np.ctypeslib.as_array(b_p, (n * nions,)))
+            return 0
+        except Exception:
+            traceback.print_exc()
+            return 1
+    fn = ASSEMBLE_FN(cb)
+    status = np.full(ncell, -99, np.int32)
+    iters = np.zeros(ncell, np.int32)
+    rc = lib.ion_populations_lockstep(ncell, nions, elem_n.size, _ptr(elem_first), _ptr(elem_n), _ptr(istate), h_elem,
+                                      _ptr(elem_dens), _ptr(ne), _ptr(den), fn, None, _ptr(status), _ptr(iters))
+    _check(rc, "ion_populations_lockstep")
+    return status, iters
 
 
 class Plan:

@@ -14,6 +14,7 @@ HEADER = Path(__file__).resolve().parent.parent / "include" / "sirocco_solve.h"
 
 def declared_functions():
     text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    text = re.sub(r"\btypedef\b[^;]*;", "", text)   # callback types are not functions
     return sorted(set(re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", text)) - {"if", "sizeof", "defined"})
 
 
