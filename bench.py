@@ -84,7 +84,7 @@ def size_class(n: int) -> str:
     for np_ in (4, 8, 12, 16, 20, 24, 28, 32):
         if n <= np_:
             return f"small{np_}"
-    for p in (48, 64, 96, 128, 160, 192, 208, 224, 256):
+    for p in (48, 64, 96, 128, 160, 192, 208, 224, 256, 320, 384, 448, 512, 640, 768, 896, 1024):
         if n <= p:
             return f"cta{p}"
     return "global"

@@ -64,7 +64,8 @@ def test_dropin_singular_leaves_output_untouched(engine):
 
 
 @pytest.mark.parametrize("sizes", [list(range(1, 33)), [33, 40, 47, 48, 50, 63, 64, 65, 80, 96, 100, 127, 128],
-                                   [129, 150, 160, 161, 178, 192, 193, 200, 208, 209, 224, 225, 256, 257]])
+                                   [129, 150, 160, 161, 178, 192, 193, 200, 208, 209, 224, 225, 256, 257],
+                                   [320, 321, 384, 385, 448, 449, 512, 513, 640, 641, 768, 769, 896, 897, 1024]])
 def test_fp64_every_size_class_matches_oracle(engine, sizes):
     rng = np.random.default_rng(sum(sizes))
     reps = 3 if max(sizes) <= 128 else 1
