@@ -201,7 +201,7 @@ small_mixed_solve_kernel(BatchView bv, MixedParams mp) {
         if (act) sm.xs[lane] = xj;
         __syncwarp(gmask);
         double worst;
-        const int code = small_residual_code<NP, G>(sm, bg, n, lane, gmask, &worst);
+        const int code = small_residual_code<NP, G>(sm, bv.A + bv.offA[s], bg, n, lane, gmask, &worst);
         // how close could the reference's own residual test come to 1e-6?
         double risk = 0.0;
         if (act) {
@@ -224,7 +224,7 @@ small_mixed_solve_kernel(BatchView bv, MixedParams mp) {
 
     int code;
     if (fallback) {
-      code = small_exact_solve<NP, G>(sm, bg, xg, n, lane, gmask);
+      code = small_exact_solve<NP, G>(sm, bv.A + bv.offA[s], bg, xg, n, lane, gmask);
       diagbits |= kDiagFallback;
     } else {
       for (int k = lane; k < n; k += G) xg[k] = sm.xs[k];

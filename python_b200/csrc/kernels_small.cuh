@@ -4,8 +4,9 @@
 // A group of G lanes (G in {4, 8, 16, 32}, so 8/4/2/1 systems per warp) owns
 // one system; lane r holds row r of A in registers (NP doubles, NP >= n, all
 // indices compile-time after unrolling).  Rows never move: each carries its
-// current position `pos`, the pivot search is a (|a|, pos) butterfly over the
-// group, and the pivot row is broadcast through a small shared buffer.
+// current position `pos`, the pivot search is three redux.sync reductions of
+// (|a| bits, position) over the group, and the pivot row is broadcast through a
+// small shared buffer.
 //
 // solve  : GSL-exact LU (lu.c:62-288), then the two row-oriented triangular
 //          sweeps of LU_svx (lu.c:329-360, cblas/source_trsv_r.h) in GSL's
@@ -81,16 +82,20 @@ __device__ __forceinline__ bool small_exact_factor(SmallSmem<NP>& sm, double (&a
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
     if (j < n && !sing) {
-      double key = (act && !done) ? pivot_key(a[j]) : -1.0;
-      int kp = pos, kl = lane;
-#pragma unroll
-      for (int off = G / 2; off > 0; off >>= 1) {
-        const double ok = __shfl_xor_sync(gmask, key, off, G);
-        const int op = __shfl_xor_sync(gmask, kp, off, G);
-        const int ol = __shfl_xor_sync(gmask, kl, off, G);
-        if (pivot_better(ok, op, key, kp)) { key = ok; kp = op; kl = ol; }
+      // first strict maximum of |a| in current row order (cblas idamax): the
+      // eligible rows' keys carry bit 63 and NaN counts as zero; ties go to the
+      // smaller position
+      const bool elig = act && !done;
+      unsigned long long key = 0ull;
+      if (elig) {
+        const double v = fabs(a[j]);
+        key = (v == v) ? (static_cast<unsigned long long>(__double_as_longlong(v)) | (1ull << 63)) : (1ull << 63);
       }
-      const int p = kl;
+      const unsigned hi = unsigned(key >> 32), lo = unsigned(key);
+      const unsigned mh = __reduce_max_sync(gmask, hi);
+      const unsigned ml = __reduce_max_sync(gmask, hi == mh ? lo : 0u);
+      const int kp = int(__reduce_min_sync(gmask, (elig && hi == mh && lo == ml) ? unsigned(pos) : 0xffffffffu));
+      const int p = (__ffs(__ballot_sync(gmask, elig && pos == kp)) - 1) & (G - 1);
       const bool was_done = done;
       if (lane == p) {
         pos = j;
@@ -139,16 +144,17 @@ __device__ __forceinline__ bool small_exact_factor(SmallSmem<NP>& sm, double (&a
 // A (sm.stage); the first failing row decides (matrix_cpu.c:162-187).  Also
 // returns, in *worst, the largest check value over all rows.
 template <int NP, int G>
-__device__ __forceinline__ int small_residual_code(SmallSmem<NP>& sm, const double* __restrict__ bg, int n,
-                                                   int lane, unsigned gmask, double* worst) {
-  constexpr int S = SmallSmem<NP>::S;
+__device__ __forceinline__ int small_residual_code(SmallSmem<NP>& sm, const double* __restrict__ Ag,
+                                                   const double* __restrict__ bg, int n, int lane, unsigned gmask,
+                                                   double* worst) {
   int code = 0;
   double chk = 0.0;
   if (lane < n) {
     double acc = 0.0;
+    const double* __restrict__ arow = Ag + lane * n;
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      if (k < n) acc = add_rn(acc, mul_rn(sm.stage[lane * S + k], sm.xs[k]));
+      if (k < n) acc = add_rn(acc, mul_rn(__ldg(arow + k), sm.xs[k]));
     const double y = add_rn(0.0, acc);
     const double bi = bg[lane];
     if (bi > 0.0) {
@@ -174,10 +180,13 @@ __device__ __forceinline__ int small_residual_code(SmallSmem<NP>& sm, const doub
   return fcode;
 }
 
-// Complete GSL-exact solve of the staged system; writes x and returns the code.
+// Complete GSL-exact solve of the staged system (Ag: the same matrix in global
+// memory, for the residual check); writes x and returns the code.  The staged
+// copy is overwritten with the factors.
 template <int NP, int G>
-__device__ __forceinline__ int small_exact_solve(SmallSmem<NP>& sm, const double* __restrict__ bg,
-                                                 double* __restrict__ xg, int n, int lane, unsigned gmask) {
+__device__ __forceinline__ int small_exact_solve(SmallSmem<NP>& sm, const double* __restrict__ Ag,
+                                                 const double* __restrict__ bg, double* __restrict__ xg, int n,
+                                                 int lane, unsigned gmask) {
   constexpr int S = SmallSmem<NP>::S;
   const bool act = lane < n;
   double a[NP];
@@ -196,22 +205,26 @@ __device__ __forceinline__ int small_exact_solve(SmallSmem<NP>& sm, const double
       if (act && pos > j) t = sub_rn(t, mul_rn(a[j], yj));
     }
   }
-  // backward sweep, row-oriented: x_i = (y_i - sum_{k>i} U_ik x_k) / U_ii
+  // backward sweep, row-oriented: x_i = (y_i - sum_{k>i} U_ik x_k) / U_ii; the
+  // rows of U go to shared memory by position and one lane walks them
+  if (act) {
 #pragma unroll
-  for (int i = NP - 1; i >= 0; --i) {
-    if (i < n) {
-      if (act && pos == i) {
-        double u = t;
-#pragma unroll
-        for (int k = i + 1; k < NP; ++k)
-          if (k < n) u = sub_rn(u, mul_rn(a[k], sm.xs[k]));
-        sm.xs[i] = div_rn(u, a[i]);
-      }
-      __syncwarp(gmask);
+    for (int k = 0; k < NP; ++k) sm.stage[pos * S + k] = a[k];
+    sm.piv[pos] = t;
+  }
+  __syncwarp(gmask);
+  if (lane == 0) {
+    for (int i = n - 1; i >= 0; --i) {
+      const double* __restrict__ urow = &sm.stage[i * S];
+      double u = sm.piv[i];
+#pragma unroll 4
+      for (int k = i + 1; k < n; ++k) u = sub_rn(u, mul_rn(urow[k], sm.xs[k]));
+      sm.xs[i] = div_rn(u, urow[i]);
     }
   }
+  __syncwarp(gmask);
   double worst;
-  const int code = small_residual_code<NP, G>(sm, bg, n, lane, gmask, &worst);
+  const int code = small_residual_code<NP, G>(sm, Ag, bg, n, lane, gmask, &worst);
   for (int k = lane; k < n; k += G) xg[k] = sm.xs[k];
   return code;
 }
@@ -237,7 +250,7 @@ small_exact_kernel(BatchView bv) {
 
     if (KIND == kSolve) {
       const int64_t ov = bv.offv[s];
-      const int code = small_exact_solve<NP, G>(sm, bv.b + ov, bv.out + ov, n, lane, gmask);
+      const int code = small_exact_solve<NP, G>(sm, bv.A + bv.offA[s], bv.b + ov, bv.out + ov, n, lane, gmask);
       if (lane == 0) {
         bv.status[s] = code;
         if (bv.diag) bv.diag[s] = kDiagExact;
