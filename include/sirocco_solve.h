@@ -137,6 +137,30 @@ int ion_populations_lockstep(int ncell, int nions, int nelem, const int *elem_fi
                              const int *istate, int h_elem, const double *elem_dens, double *ne, double *den,
                              sirocco_ion_assemble_fn assemble, void *user, int *status, int *iters);
 
+/* Macro-atom level populations of one macro element for ncell cells at once:
+   the loop of macro_pops (source/macro_gov.c:336-505), one batched solve per
+   round over every unfinished cell.  The element has n levels in matrix order
+   (the reference's conf_to_matrix already applied) and nion ions, ion q owning
+   levels ion_first[q] .. ion_first[q]+ion_nlte[q]-1; g[n] are the levels'
+   statistical weights and radiative[lo*n+up] != 0 marks a radiative link
+   between levels lo < up.  scale[c] turns a cell's fractional ion population
+   into a density (ele[].abun * rho * rho2nh).  Each round the library calls
+   `assemble` for the unfinished cells: it fills each listed cell's n x n rate
+   matrix (macro_pops_fill_rate_matrix) into A, cell after cell, using dilute
+   estimators when attempt[i] > 1 (get_dilute_estimators after a numerical
+   error).  The library then replaces the first row with ones, solves with
+   b = e_0, zeroes populations below DENSITY_MIN, clears population inversions
+   (upper > lower * g_up / g_lo * 0.999999 on linked levels, macro_gov.c:771),
+   and accepts the cell unless an ion density or level population is negative or
+   non-finite (:823); a singular system gives the reference's zero populations.
+   pop[c*n + k] receives the accepted populations; status[c] is 0, or -2 when
+   200 rounds never produced acceptable populations; iters[c] counts rounds.
+   All arrays are host arrays. */
+typedef int (*sirocco_macro_assemble_fn)(void *user, int ncell, const int *cells, const int *attempt, double *A);
+int macro_pops_lockstep(int ncell, int n, int nion, const int *ion_first, const int *ion_nlte, const double *g,
+                        const unsigned char *radiative, const double *scale, sirocco_macro_assemble_fn assemble,
+                        void *user, double *pop, int *status, int *iters);
+
 /* Macro-atom jumping matrices of a whole cycle (the reference's
    calc_matom_matrix, source/macro_accelerate.c:311-334, called per cell from
    calc_all_matom_matrices :1054-1061).  For every cell s, N_s = I - Q/Q_norm

@@ -898,6 +898,103 @@ static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_fir
   return 0;
 }
 
+// --------------------------------------------------------- macro-atom pops --
+// macro_pops (source/macro_gov.c:336-505) for one macro element over many cells:
+// each round solves the level systems of every unfinished cell in one batched
+// call, then applies the reference's post-processing per cell.
+static int run_macro_pops(int ncell, int n, int nion, const int* ion_first, const int* ion_nlte, const double* g,
+                          const unsigned char* radiative, const double* scale, sirocco_macro_assemble_fn assemble,
+                          void* user, double* pop, int* status, int* iters) {
+  if (ncell == 0) return 0;
+  if (ncell < 0 || n < 1 || n > SIROCCO_MAX_N || nion < 1 || !ion_first || !ion_nlte || !g || !radiative ||
+      !scale || !assemble || !pop || !status || !iters) {
+    set_error("invalid macro_pops arguments");
+    return SIROCCO_EINVAL;
+  }
+  for (int q = 0; q < nion; ++q)
+    if (ion_first[q] < 0 || ion_nlte[q] < 0 || ion_first[q] + ion_nlte[q] > n) {
+      set_error("ion %d: levels [%d, %d) outside 0..%d", q, ion_first[q], ion_first[q] + ion_nlte[q], n);
+      return SIROCCO_EINVAL;
+    }
+  std::vector<int> active(ncell), attempt(ncell, 1);
+  for (int c = 0; c < ncell; ++c) {
+    active[c] = c;
+    status[c] = -2;
+    iters[c] = 0;
+  }
+  const int64_t nn = int64_t(n) * n;
+  std::vector<double> A, b, x;
+  std::vector<int> nv, st, att;
+  std::vector<int64_t> offA, offv;
+  for (int it = 1; it <= kMaxIterations && !active.empty(); ++it) {
+    const int na = int(active.size());
+    att.resize(na);
+    for (int i = 0; i < na; ++i) att[i] = attempt[active[i]];
+    A.assign(size_t(na) * nn, 0.0);
+    const int arc = assemble(user, na, active.data(), att.data(), A.data());
+    if (arc != 0) {
+      set_error("assembly callback returned %d", arc);
+      return SIROCCO_EINVAL;
+    }
+    // normalisation constraint in the first row, b = e_0 (macro_gov.c:401-404, 431)
+    b.assign(size_t(na) * n, 0.0);
+    nv.assign(na, n);
+    offA.resize(na);
+    offv.resize(na);
+    for (int i = 0; i < na; ++i) {
+      for (int k = 0; k < n; ++k) A[size_t(i) * nn + k] = 1.0;
+      b[size_t(i) * n] = 1.0;
+      offA[i] = int64_t(i) * nn;
+      offv[i] = int64_t(i) * n;
+    }
+    x.assign(size_t(na) * n, 0.0);
+    st.assign(na, 0);
+    int rc = run_batched(kSolve, na, nv.data(), offA.data(), A.data(), offv.data(), b.data(), x.data(), st.data(),
+                         ctx()->mode);
+    if (rc) return rc;
+    std::vector<int> next;
+    for (int i = 0; i < na; ++i) {
+      const int c = active[i];
+      double* p = &x[size_t(i) * n];
+      iters[c] = it;
+      // a singular system leaves the reference's zero-filled populations
+      if (st[i] == kSolveSingular) std::fill(p, p + n, 0.0);
+      for (int k = 0; k < n; ++k)
+        if (p[k] < kDensityMin) p[k] = 0.0;
+      // population inversions between radiatively linked levels (macro_gov.c:771-804)
+      for (int q = 0; q < nion; ++q) {
+        const int f = ion_first[q], e = ion_first[q] + ion_nlte[q];
+        for (int lo = f; lo < e; ++lo)
+          for (int up = lo + 1; up < e; ++up)
+            if (radiative[size_t(lo) * n + up]) {
+              const double test = p[lo] * g[up] / g[lo] * 0.999999;
+              if (p[up] > test) p[up] = test;
+            }
+      }
+      // negative or non-finite ion densities or level populations (macro_gov.c:823-865)
+      bool bad = false;
+      for (int q = 0; q < nion; ++q) {
+        const int f = ion_first[q], e = ion_first[q] + ion_nlte[q];
+        double dens = 0.0;
+        for (int k = f; k < e; ++k) dens += p[k];
+        const double d = dens * scale[c];
+        if (!std::isfinite(d) || d < 0.0) bad = true;
+        for (int k = f; k < e; ++k)
+          if (p[k] < 0.0 || !std::isfinite(p[k])) bad = true;
+      }
+      if (!bad) {
+        status[c] = 0;
+        std::copy(p, p + n, pop + size_t(c) * n);
+      } else if (it < kMaxIterations) {
+        attempt[c] = it + 1;   // the caller re-assembles with dilute estimators
+        next.push_back(c);
+      }
+    }
+    active.swap(next);
+  }
+  return 0;
+}
+
 // single system through the host path, honouring the reference's "output
 // untouched on a singular matrix" behaviour
 static int run_single(int kind, double* A, const double* b, int size, double* out, int* code) {
@@ -1101,6 +1198,13 @@ int ion_populations_lockstep(int ncell, int nions, int nelem, const int* elem_fi
                              sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
   return ss::run_ion_lockstep(ncell, nions, nelem, elem_first, elem_n, istate, h_elem, elem_dens, ne, den, assemble,
                               user, status, iters);
+}
+
+int macro_pops_lockstep(int ncell, int n, int nion, const int* ion_first, const int* ion_nlte, const double* g,
+                        const unsigned char* radiative, const double* scale, sirocco_macro_assemble_fn assemble,
+                        void* user, double* pop, int* status, int* iters) {
+  return ss::run_macro_pops(ncell, n, nion, ion_first, ion_nlte, g, radiative, scale, assemble, user, pop, status,
+                            iters);
 }
 
 int solve_matrix_batched_noalloc(int nsys, int nmax, const int* n, const int64_t* offA, const double* A,

@@ -29,12 +29,13 @@ EXPORTS = (
     "solve_matrix_batched", "invert_matrix_batched", "sirocco_set_precision",
     "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
     "sirocco_plan_destroy", "sirocco_last_error", "solve_matrix_batched_noalloc",
-    "matom_matrices_batched", "matom_sample_batched", "ion_populations_lockstep",
+    "matom_matrices_batched", "matom_sample_batched", "ion_populations_lockstep", "macro_pops_lockstep",
 )
 
 _lib = None
 
 # assembly callback of ion_populations_lockstep
+MACRO_ASSEMBLE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_int, POINTER(c_int), POINTER(c_int), POINTER(c_double))
 ASSEMBLE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_double),
                                POINTER(c_double), POINTER(c_double), POINTER(c_double))
 
@@ -89,6 +90,9 @@ def load() -> ctypes.CDLL:
     lib.ion_populations_lockstep.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                                              c_void_p, c_void_p, ASSEMBLE_FN, c_void_p, c_void_p, c_void_p]
     lib.ion_populations_lockstep.restype = c_int
+    lib.macro_pops_lockstep.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        MACRO_ASSEMBLE_FN, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.macro_pops_lockstep.restype = c_int
     _lib = lib
     return lib
 
@@ -239,6 +243,40 @@ def ion_populations_lockstep(elem_first, elem_n, istate, h_elem: int, elem_dens:
                                       _ptr(elem_dens), _ptr(ne), _ptr(den), fn, None, _ptr(status), _ptr(iters))
     _check(rc, "ion_populations_lockstep")
     return status, iters
+
+
+def macro_pops_lockstep(ion_first, ion_nlte, g, radiative: np.ndarray, scale: np.ndarray, ncell: int, assemble):
+    """Level populations of one macro element in every cell (macro_pops_lockstep).
+
+    ``assemble(cells, attempt, A)`` fills, in place, the n x n rate matrices
+    of the listed cells (A packed cell after cell).  Returns (pop [ncell, n],
+    status, iters).
+    """
+    import traceback
+    lib = load()
+    ion_first = np.ascontiguousarray(ion_first, np.int32)
+    ion_nlte = np.ascontiguousarray(ion_nlte, np.int32)
+    g = np.ascontiguousarray(g, np.float64)
+    rad = np.ascontiguousarray(radiative, np.uint8)
+    scale = np.ascontiguousarray(scale, np.float64)
+    n = g.size
+
+    def cb(user, k, cells, att, a_p):
+        try:
+            assemble(np.ctypeslib.as_array(cells, (k,)).copy(), np.ctypeslib.as_array(att, (k,)).copy(),
+                     np.ctypeslib.as_array(a_p, (k * n * n,)))
+            return 0
+        except Exception:
+            traceback.print_exc()
+            return 1
+    fn = MACRO_ASSEMBLE_FN(cb)
+    pop = np.full((ncell, n), np.nan)
+    status = np.full(ncell, -99, np.int32)
+    iters = np.zeros(ncell, np.int32)
+    rc = lib.macro_pops_lockstep(ncell, n, ion_first.size, _ptr(ion_first), _ptr(ion_nlte), _ptr(g), _ptr(rad),
+                                 _ptr(scale), fn, None, _ptr(pop), _ptr(status), _ptr(iters))
+    _check(rc, "macro_pops_lockstep")
+    return pop, status, iters
 
 
 class Plan:
