@@ -18,7 +18,7 @@ LIB = PKG / "libsirocco_solve.so"
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = [CSRC / "engine.cu"]
-HEADERS = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "sirocco_solve.h"]
+HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + [ROOT / "include" / "sirocco_solve.h"]
 
 
 def _stale(target: Path, deps) -> bool:

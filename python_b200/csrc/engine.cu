@@ -65,8 +65,13 @@ struct KernelSpec {
 
 // size classes of the small family (padded row length NP, lanes per system G)
 static const int kSmallNP[] = {4, 8, 12, 16, 20, 24, 28, 32};
-static const int kCtaP[] = {48, 64, 96, 128, 160, 192, 208, 224, 256, 320, 384, 448, 512, 640, 768, 896, 1024};
-constexpr int kCtaClasses = 17;
+// padded orders of the CTA classes (cta_classes.inc, chosen by python_b200/autotune.py)
+static const int kCtaP[] = {
+#define SS_CTA_CLASS(I, P, NT, RG, CC, PW, GM, MINB) P,
+#include "cta_classes.inc"
+#undef SS_CTA_CLASS
+};
+constexpr int kCtaClasses = int(sizeof(kCtaP) / sizeof(kCtaP[0]));
 
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
@@ -108,7 +113,7 @@ static KernelSpec small_spec(int cls, int mode) {
 template <int KIND>
 static KernelSpec cta_spec(int cls) {
   KernelSpec k;
-#define SS_CTA(I, P, NT, RG, CC, PW, GM, MINB)                                          \
+#define SS_CTA_CLASS(I, P, NT, RG, CC, PW, GM, MINB)                                    \
   case I: {                                                                             \
     using Sh = CtaShape<KIND, P, NT, RG, CC, PW, GM, MINB>;                             \
     k.fn = reinterpret_cast<const void*>(&cta_exact_kernel<KIND, P, NT, RG, CC, PW, GM, MINB>); \
@@ -117,33 +122,14 @@ static KernelSpec cta_spec(int cls) {
     k.work_slab = Sh::slab;                                                             \
     break;                                                                              \
   }
-  // order classes up to 64 keep the matrix in shared memory; above, in a
-  // global workspace slab per CTA, where more CTAs per SM (more pivot chains in
-  // flight) beat the faster memory: measured on B200, n = 90 / 120 / 150
-  // inverses ran 1.1x / 1.6x / 1.3x faster from L2 than from shared memory
+  // the class table, measured per class by python_b200/autotune.py: shared
+  // memory for the smallest orders, a global workspace slab above them, where
+  // more CTAs per SM (more pivot chains in flight) beat the faster memory
   switch (cls) {
-    SS_CTA(0, 48, 96, 2, 6, 1, false, 0)
-    SS_CTA(1, 64, 128, 2, 8, 1, false, 0)
-    SS_CTA(2, 96, 128, 2, 6, 2, true, 4)
-    SS_CTA(3, 128, 128, 2, 8, 2, true, 4)
-    SS_CTA(4, 160, 160, 2, 10, 3, true, 3)
-    SS_CTA(5, 192, 256, 2, 8, 3, true, 2)
-    SS_CTA(6, 208, 416, 2, 13, 4, true, 1)
-    SS_CTA(7, 224, 224, 2, 7, 4, true, 2)
-    SS_CTA(8, 256, 256, 2, 8, 4, true, 2)
-    // one CTA of 16 warps per SM, all of them panel warps: n = 500 / 1000
-    // inverses ran 1.4x / 1.6x faster than on the global-memory kernel
-    SS_CTA(9, 320, 320, 2, 8, 8, true, 1)
-    SS_CTA(10, 384, 512, 2, 8, 8, true, 1)
-    SS_CTA(11, 448, 448, 2, 8, 8, true, 1)
-    SS_CTA(12, 512, 512, 2, 8, 8, true, 1)
-    SS_CTA(13, 640, 512, 2, 8, 8, true, 1)
-    SS_CTA(14, 768, 512, 2, 8, 8, true, 1)
-    SS_CTA(15, 896, 512, 2, 8, 8, true, 1)
-    SS_CTA(16, 1024, 512, 2, 8, 8, true, 1)
+#include "cta_classes.inc"
     default: break;
   }
-#undef SS_CTA
+#undef SS_CTA_CLASS
   return k;
 }
 

@@ -1,0 +1,27 @@
+"""The CTA class table the engine compiles in (python_b200/csrc/cta_classes.inc)
+is a valid autotuner result: ascending orders, each class one of the timed
+candidates, and in agreement with the tuner's record when there is one."""
+import json
+
+from python_b200 import autotune
+
+
+def test_class_table_comes_from_the_candidates():
+    classes = autotune.parse_classes()
+    cands = set(autotune.parse_candidates())
+    orders = [c[0] for c in classes]
+    assert orders == sorted(set(orders)) and orders[0] > 32
+    assert orders[-1] >= 1024                      # every supported order has a class
+    for c in classes:
+        assert c in cands, c
+
+
+def test_record_matches_table():
+    if not autotune.RECORD.exists():
+        return
+    rec = json.loads(autotune.RECORD.read_text())
+    table = {c[0]: c for c in autotune.parse_classes()}
+    for entry in rec["classes"]:
+        assert tuple(entry["chosen"]) == table[entry["P"]], entry["P"]
+        timed = [tuple(c["config"]) for c in entry["candidates"] if "ms" in c]
+        assert tuple(entry["chosen"]) in timed
