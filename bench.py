@@ -425,6 +425,55 @@ def run_ours(args):
     value = aggregate(world, nsys_step, args.steps, t)
     launches = sum(p.launches for p in plans) * args.steps
 
+    # ---- mixed sizes: the same step as one graph launch, and as one launch per size
+    launch_modes = None
+    if world == 1 and any(len(np.unique(b.n)) > 1 for b in batches):
+        side = torch.cuda.Stream(device)
+        graph = torch.cuda.CUDAGraph()
+        side.wait_stream(stream)
+        with torch.cuda.graph(graph, stream=side):
+            for p, (A, bb, out, st, diag) in zip(plans, bufs):
+                p.execute(A, out, st, b=bb, diag=diag, stream=side)
+        torch.cuda.synchronize(device)
+        for _ in range(2):
+            graph.replay()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            graph.replay()
+        g1.record(stream)
+        torch.cuda.synchronize(device)
+        t_graph = g0.elapsed_time(g1) / 1e3 / args.steps
+        # one plan (one kernel launch) per distinct order, over the same buffers
+        per_size = []
+        for b, m, (A, bb, out, st, diag) in zip(batches, modes, bufs):
+            for nval in np.unique(b.n):
+                idx = np.nonzero(b.n == nval)[0]
+                sub = wl.Batch(b.kind, b.n[idx], b.offA[idx], b.A, b.offv[idx] if b.kind == "solve" else None, b.b)
+                per_size.append((engine.Plan(sub, code[m]), (A, bb, out, st, diag)))
+        one = sum(p.launches for p, _ in per_size)
+
+        def per_size_step():
+            for p, (A, bb, out, st, diag) in per_size:
+                p.execute(A, out, st, b=bb, diag=diag, stream=stream)
+        for _ in range(2):
+            per_size_step()
+        torch.cuda.synchronize(device)
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(args.steps):
+            per_size_step()
+        q1.record(stream)
+        torch.cuda.synchronize(device)
+        t_per = q0.elapsed_time(q1) / 1e3 / args.steps
+        for p, _ in per_size:
+            p.close()
+        del graph
+        launch_modes = {"bucketed_plans_ms": 1e3 * t / args.steps,
+                        "bucketed_launches_per_step": sum(p.launches for p in plans),
+                        "graph_replay_ms": 1e3 * t_graph, "graph_launches_per_step": 1,
+                        "one_launch_per_size_ms": 1e3 * t_per, "one_launch_per_size_launches": one}
+
     # ---- accuracy of what was timed ------------------------------------
     acc = []
     for b, m, (A, bb, out, st, diag) in zip(batches, modes, bufs):
@@ -586,7 +635,8 @@ def run_ours(args):
                 "accuracy": acc, "plain_fp64_value": fp64_value,
                 "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
                 "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
-                "cusolver_reference": cus, "gpu_launches": launches, "clocks": clock_info}
+                "cusolver_reference": cus, "launch_modes": launch_modes, "gpu_launches": launches,
+                "clocks": clock_info}
         print(json.dumps(line), flush=True)
     for p in plans:
         p.close()

@@ -418,8 +418,14 @@ struct Pipeline {
   }
 };
 
-constexpr int kPipeStreams = 4;
-constexpr int64_t kChunkBytes = int64_t(16) << 20;
+#ifndef SS_CHUNK_MIB
+#define SS_CHUNK_MIB 16   // host pipeline chunk size
+#endif
+#ifndef SS_PIPE_STREAMS
+#define SS_PIPE_STREAMS 4 // host pipeline streams
+#endif
+constexpr int kPipeStreams = SS_PIPE_STREAMS;
+constexpr int64_t kChunkBytes = int64_t(SS_CHUNK_MIB) << 20;
 
 struct Context {
   int device = -1;
