@@ -425,6 +425,8 @@ struct Pipeline {
 #define SS_PIPE_STREAMS 4 // host pipeline streams
 #endif
 constexpr int kPipeStreams = SS_PIPE_STREAMS;
+constexpr size_t kPlanCache = 16;                      // plans cached per thread
+constexpr int64_t kPlanWorkBytes = int64_t(8) << 30;   // workspace the cached plans may hold
 constexpr int64_t kChunkBytes = int64_t(SS_CHUNK_MIB) << 20;
 
 struct Context {
@@ -532,12 +534,23 @@ struct Context {
     const uint64_t h = layout_hash(kind, md, nsys, n, offA, offv);
     auto it = plans.find(h);
     if (it != plans.end()) {
+      // most recently used last
+      plan_order.erase(std::find(plan_order.begin(), plan_order.end(), h));
+      plan_order.push_back(h);
       *out = it->second;
       return 0;
     }
     int rc = plan_build(out, kind, nsys, n, offA, offv, md);
     if (rc) return rc;
-    if (plan_order.size() >= 16) {
+    // at most kPlanCache plans, and no more than kPlanWorkBytes of workspace
+    // held by cached plans besides the new one: least recently used go first
+    auto held = [&]() {
+      int64_t b = 0;
+      for (auto& kv : plans) b += kv.second->scratch_elems * int64_t(sizeof(double));
+      return b;
+    };
+    while (!plan_order.empty() && (plan_order.size() >= kPlanCache ||
+                                   held() + (*out)->scratch_elems * int64_t(sizeof(double)) > kPlanWorkBytes)) {
       auto old = plans.find(plan_order.front());
       if (old != plans.end()) {
         plan_free(old->second);

@@ -46,8 +46,9 @@ __device__ __forceinline__ void panel_bar(int count) { asm volatile("bar.sync 1,
 
 constexpr int kSmemPerSm = 233472;   // shared memory of one SM (228 KB)
 
-// P: padded order; NT: threads; RG x CC: rows x columns of one update tile
-// (columns tc + 8c); PW: panel warps; GM: matrix in a global workspace slab;
+// P: padded order; NT: threads; RG x CC: rows x columns of one update tile of
+// the workspace classes (columns tc + 8c; the shared-memory classes update one
+// column at a time); PW: panel warps; GM: matrix in a global workspace slab;
 // MINB: CTAs per SM asked of the register allocator (0: as many as fit).
 template <int KIND, int P_, int NT_, int RG_, int CC_, int PW_, bool GM_, int MINB_>
 struct CtaShape {
@@ -367,45 +368,114 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
       __syncthreads();
 
       // ---- 3. update of every other row outside the panel ----------------------
+      if (!GM) {
+        // Shared memory: column by column.  The panel's own columns are
+        // skipped, a solve skips its L columns too, and the inverse's columns
+        // left of the panel (the Gauss-Jordan inverse, never part of GSL's LU)
+        // take fused updates; every other entry gets GSL's unfused
+        // multiply-subtract with k ascending.
 #pragma unroll 1
-      for (int rg = 0; rg < RB; rg += RG) {
-        int row[RG];
-        bool keep[RG];
-#pragma unroll
-        for (int u = 0; u < RG; ++u) {
-          row[u] = tr + TGR * (rg + u);
-          const int p = ps_s[row[u]];
-          keep[u] = row[u] < n && (p < j0 || p >= j0 + nb) && (KIND == kInvert || p >= j0 + B);
-        }
-#pragma unroll 1
-        for (int cg = 0; cg < CB; cg += CC) {
-          double a[RG][CC];
+        for (int rg = 0; rg < RB; rg += RG) {
+          int row[RG], sw[RG];
+          bool keep[RG];
+          double mk[B][RG];
 #pragma unroll
           for (int u = 0; u < RG; ++u) {
-            const int sw = cta_swz(row[u]);
+            row[u] = tr + TGR * (rg + u);
+            sw[u] = cta_swz(row[u]);
+            const int p = ps_s[row[u]];
+            keep[u] = row[u] < n && (p < j0 || p >= j0 + nb) && (KIND == kInvert || p >= j0 + B);
 #pragma unroll
-            for (int c = 0; c < CC; ++c) a[u][c] = M[row[u] * P + ((tc + 8 * (cg + c)) ^ sw)];
+            for (int k = 0; k < B; ++k) mk[k][u] = Mm[row[u] * MS + k];
           }
+#pragma unroll 2
+          for (int c = 0; c < CB; ++c) {
+            if (c == jb || (KIND == kSolve && c < jb)) continue;
+            const int col = tc + 8 * c;
+            double vk[B], a[RG];
 #pragma unroll
-          for (int k = 0; k < B; ++k) {
-            double mk[RG], vk[CC];
+            for (int k = 0; k < B; ++k) vk[k] = Vs[k * P + col];
 #pragma unroll
-            for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
+            for (int u = 0; u < RG; ++u) a[u] = M[row[u] * P + (col ^ sw[u])];
+            if (KIND == kInvert && c < jb) {
 #pragma unroll
-            for (int c = 0; c < CC; ++c) vk[c] = Vs[k * P + tc + 8 * (cg + c)];
+              for (int k = 0; k < B; ++k)
+#pragma unroll
+                for (int u = 0; u < RG; ++u) a[u] = fma(-mk[k][u], vk[k], a[u]);
+            } else {
+#pragma unroll
+              for (int k = 0; k < B; ++k)
+#pragma unroll
+                for (int u = 0; u < RG; ++u) a[u] = sub_rn(a[u], mul_rn(mk[k][u], vk[k]));
+            }
 #pragma unroll
             for (int u = 0; u < RG; ++u)
-#pragma unroll
-              for (int c = 0; c < CC; ++c) a[u][c] = sub_rn(a[u][c], mul_rn(mk[u], vk[c]));
+              if (keep[u]) M[row[u] * P + (col ^ sw[u])] = a[u];
           }
+        }
+      } else {
+        // Global workspace: RG x CC tiles, every load of a tile in flight
+        // together to cover the L2 latency; GSL's unfused multiply-subtract
+        // with k ascending except on tiles wholly left of the panel.
+#pragma unroll 1
+        for (int rg = 0; rg < RB; rg += RG) {
+          int row[RG];
+          bool keep[RG];
 #pragma unroll
           for (int u = 0; u < RG; ++u) {
-            if (keep[u]) {
+            row[u] = tr + TGR * (rg + u);
+            const int p = ps_s[row[u]];
+            keep[u] = row[u] < n && (p < j0 || p >= j0 + nb) && (KIND == kInvert || p >= j0 + B);
+          }
+#pragma unroll 1
+          for (int cg = 0; cg < CB; cg += CC) {
+            // a chunk wholly left of the panel: fused updates for an inverse
+            // (outside GSL's LU), nothing to do for a solve (its L columns)
+            const bool left = cg + CC <= jb;
+            if (KIND == kSolve && left) continue;
+            double a[RG][CC];
+#pragma unroll
+            for (int u = 0; u < RG; ++u) {
               const int sw = cta_swz(row[u]);
 #pragma unroll
-              for (int c = 0; c < CC; ++c) {
-                const int cb = cg + c;
-                if (cb != jb && (KIND == kInvert || cb > jb)) M[row[u] * P + ((tc + 8 * cb) ^ sw)] = a[u][c];
+              for (int c = 0; c < CC; ++c) a[u][c] = M[row[u] * P + ((tc + 8 * (cg + c)) ^ sw)];
+            }
+            if (left) {
+#pragma unroll
+              for (int k = 0; k < B; ++k) {
+                double mk[RG], vk[CC];
+#pragma unroll
+                for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
+#pragma unroll
+                for (int c = 0; c < CC; ++c) vk[c] = Vs[k * P + tc + 8 * (cg + c)];
+#pragma unroll
+                for (int u = 0; u < RG; ++u)
+#pragma unroll
+                  for (int c = 0; c < CC; ++c) a[u][c] = fma(-mk[u], vk[c], a[u][c]);
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < B; ++k) {
+                double mk[RG], vk[CC];
+#pragma unroll
+                for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
+#pragma unroll
+                for (int c = 0; c < CC; ++c) vk[c] = Vs[k * P + tc + 8 * (cg + c)];
+#pragma unroll
+                for (int u = 0; u < RG; ++u)
+#pragma unroll
+                  for (int c = 0; c < CC; ++c) a[u][c] = sub_rn(a[u][c], mul_rn(mk[u], vk[c]));
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < RG; ++u) {
+              if (keep[u]) {
+                const int sw = cta_swz(row[u]);
+#pragma unroll
+                for (int c = 0; c < CC; ++c) {
+                  const int cb = cg + c;
+                  if (cb != jb && (KIND == kInvert || cb > jb)) M[row[u] * P + ((tc + 8 * cb) ^ sw)] = a[u][c];
+                }
               }
             }
           }
