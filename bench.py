@@ -560,16 +560,31 @@ def run_ours(args):
         for _ in range(max(1, args.warmup // 2)):
             e2e_step()
         torch.cuda.synchronize(device)
-        barrier(dist, device)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
-        torch.cuda.synchronize(device)
-        te = reduce_max(dist, time.perf_counter() - t0, device)
-        barrier(dist, device)
+
+        def e2e_block():
+            barrier(dist, device)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step()
+            torch.cuda.synchronize(device)
+            te_ = reduce_max(dist, time.perf_counter() - t0, device)
+            barrier(dist, device)
+            return te_
+
+        # a wall-clock window of a few milliseconds is at the mercy of one host
+        # hiccup: short runs repeat the K-step block (every rank the same count)
+        # and keep the median block
+        blocks = [e2e_block()]
+        reps = int(min(9, max(1, 0.3 // max(blocks[0], 1e-6))))
+        if dist is not None:
+            reps = int(reduce_max(dist, float(reps), device))
+        blocks += [e2e_block() for _ in range(reps - 1)]
+        te = statistics.median(blocks)
         e2e = {"value": world * nsys_step * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h),
-               "path": "solve_matrix_batched / invert_matrix_batched with pinned host buffers, wall clock"}
+               "d2h_bytes_per_step": int(d2h), "blocks": len(blocks),
+               "block_s_min_max": [min(blocks), max(blocks)],
+               "path": "solve_matrix_batched / invert_matrix_batched with pinned host buffers, wall clock, "
+                       "median of the K-step blocks"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -155,6 +155,10 @@ def main(argv=None) -> int:
             f"{dict(mine)[i][1:]}={scores[i]:.2f}ms" for i in good) + f"  -> {best[p]}", flush=True)
     if args.dry_run:
         return 0
+    if args.only and RECORD.exists():
+        # classes not re-tuned keep their earlier timings in the record
+        kept = [e for e in json.loads(RECORD.read_text()).get("classes", []) if e["P"] not in args.only]
+        record["classes"] = sorted(kept + record["classes"], key=lambda e: e["P"])
     write_outputs(best, record)
     if not args.no_build:
         build.build_engine(force=True)
