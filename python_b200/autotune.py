@@ -67,6 +67,41 @@ def build_tune_lib() -> Path:
     return TUNE_LIB
 
 
+def load_tune_lib():
+    """The tuning library with its argument types, and its candidates as
+    (index, (P, threads, RG, CC, panel warps, global memory, CTAs per SM asked))."""
+    lib = ctypes.CDLL(str(build_tune_lib()))
+    lib.sirocco_tune_info.argtypes = [c_int, POINTER(c_int)]
+    lib.sirocco_tune_time.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                      POINTER(c_float), POINTER(c_int)]
+    cands = []
+    for i in range(lib.sirocco_tune_count()):
+        cfg = (c_int * 7)()
+        lib.sirocco_tune_info(i, cfg)
+        cands.append((i, tuple(cfg[:5]) + (bool(cfg[5]), cfg[6])))
+    return lib, cands
+
+
+def run_candidate(lib, i: int, batch, device, reps: int = 1):
+    """Inverts a device copy of the batch with candidate i; returns (out, status, ms, CTAs per SM)."""
+    import torch
+    nsys = batch.nsys
+    dn = torch.from_numpy(np.ascontiguousarray(batch.n, np.int32)).to(device)
+    doff = torch.from_numpy(np.ascontiguousarray(batch.offA, np.int64)).to(device)
+    dA = torch.from_numpy(batch.A).to(device)
+    dlist = torch.arange(nsys, dtype=torch.int32, device=device)
+    out = torch.empty_like(dA)
+    st = torch.full((nsys,), -99, dtype=torch.int32, device=device)
+    ms, res = c_float(), c_int()
+    rc = lib.sirocco_tune_time(i, nsys, c_void_p(dn.data_ptr()), c_void_p(doff.data_ptr()), c_void_p(dA.data_ptr()),
+                               c_void_p(out.data_ptr()), c_void_p(st.data_ptr()), c_void_p(dlist.data_ptr()), reps,
+                               ctypes.byref(ms), ctypes.byref(res))
+    torch.cuda.synchronize(device)
+    if rc != 0:
+        return None, None, rc, 0
+    return out.cpu().numpy(), st.cpu().numpy(), ms.value, res.value
+
+
 def test_orders(p: int, p_prev: int):
     lo = max(p_prev + 1, SMALLEST_CTA_ORDER)
     return sorted({(lo + p) // 2, p - max(1, (p - lo) // 8)})
@@ -93,15 +128,7 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     import torch
 
-    lib = ctypes.CDLL(str(build_tune_lib()))
-    lib.sirocco_tune_info.argtypes = [c_int, POINTER(c_int)]
-    lib.sirocco_tune_time.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
-                                      POINTER(c_float), POINTER(c_int)]
-    cands = []
-    for i in range(lib.sirocco_tune_count()):
-        cfg = (c_int * 7)()
-        lib.sirocco_tune_info(i, cfg)
-        cands.append((i, tuple(cfg[:5]) + (bool(cfg[5]), cfg[6])))
+    lib, cands = load_tune_lib()
     orders = sorted({c[1][0] for c in cands})
     current = {c[0]: c for c in parse_classes()}
     best = {p: current[p] for p in current if p in orders}
@@ -119,33 +146,21 @@ def main(argv=None) -> int:
         for n in entry["orders"]:
             nsys = int(min(8192, max(296, WORK_FLOP / (2.0 * n ** 3)), MAX_BYTES // (8 * n * n)))
             batch = wl.macro_batch([n] * nsys, seed=1000 + n, density=0.25 if n <= 256 else 0.10)
-            dn = torch.from_numpy(np.ascontiguousarray(batch.n, np.int32)).to(dev)
-            doff = torch.from_numpy(np.ascontiguousarray(batch.offA, np.int64)).to(dev)
-            dA = torch.from_numpy(batch.A).to(dev)
-            dlist = torch.arange(nsys, dtype=torch.int32, device=dev)
             ref = None
             for i, cfg in mine:
-                out = torch.empty_like(dA)
-                st = torch.full((nsys,), -99, dtype=torch.int32, device=dev)
-                ms, res = c_float(), c_int()
-                rc = lib.sirocco_tune_time(i, nsys, c_void_p(dn.data_ptr()), c_void_p(doff.data_ptr()),
-                                           c_void_p(dA.data_ptr()), c_void_p(out.data_ptr()), c_void_p(st.data_ptr()),
-                                           c_void_p(dlist.data_ptr()), args.reps, ctypes.byref(ms), ctypes.byref(res))
-                torch.cuda.synchronize()
-                if rc != 0:
+                out, st, ms, res = run_candidate(lib, i, batch, dev, args.reps)
+                if out is None:
                     ok[i] = False
-                    entry["candidates"].append({"config": cfg, "n": n, "error": rc})
+                    entry["candidates"].append({"config": cfg, "n": n, "error": ms})
                     continue
-                got = (out.cpu().numpy().tobytes(), st.cpu().numpy().tobytes())
+                got = (out.tobytes(), st.tobytes())
                 if ref is None:
                     ref = got
                 elif got != ref:
                     raise SystemExit(f"candidate {cfg} disagrees with {mine[0][1]} at n={n}")
-                scores[i] += ms.value
-                entry["candidates"].append({"config": cfg, "n": n, "nsys": nsys, "ms": ms.value,
-                                            "ctas_per_sm": res.value,
-                                            "tflops": 2.0 * n ** 3 * nsys / (ms.value * 1e-3) / 1e12})
-            del dA, dn, doff, dlist
+                scores[i] += ms
+                entry["candidates"].append({"config": cfg, "n": n, "nsys": nsys, "ms": ms, "ctas_per_sm": res,
+                                            "tflops": 2.0 * n ** 3 * nsys / (ms * 1e-3) / 1e12})
         good = [i for i, _ in mine if ok[i]]
         win = min(good, key=lambda i: scores[i])
         best[p] = dict(mine)[win]

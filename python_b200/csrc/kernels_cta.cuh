@@ -165,7 +165,10 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
         // pivot search reads; its other columns are updated at the start of the
         // next step, while that step's reduction is in flight.  dmode: 0 nothing
         // pending, 1 subtract dl * dpv, 2 scale by drinv (the pivot row); dpv is
-        // the pending step's pivot row in that step's register frame.
+        // the pending step's pivot row in that step's register frame.  The
+        // pivot row's registers hold dpv itself, so its scaled values are the
+        // same for every lane, and each row takes its new value by selection:
+        // no lane-dependent branches in the panel.
         int dmode[RPL];
         double dl[RPL], dpv[B];
         double drinv = 0.0;
@@ -175,13 +178,16 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
 #pragma unroll
         for (int c = 0; c < B; ++c) dpv[c] = 0.0;
         auto apply_pending = [&]() {
+          double sv[B];
+#pragma unroll
+          for (int c = 2; c < B; ++c) sv[c] = (KIND == kInvert) ? mul_rn(dpv[c], drinv) : 0.0;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
 #pragma unroll
             for (int c = 2; c < B; ++c) {
-              if (dmode[i] == 1 && (KIND == kInvert || dk + c < B))
-                pr[i][c - 1] = sub_rn(pr[i][c - 1], mul_rn(dl[i], dpv[c]));
-              if (KIND == kInvert && dmode[i] == 2) pr[i][c - 1] = mul_rn(pr[i][c - 1], drinv);
+              const double x = sub_rn(pr[i][c - 1], mul_rn(dl[i], dpv[c]));
+              if (KIND == kInvert) pr[i][c - 1] = dmode[i] == 2 ? sv[c] : (dmode[i] == 1 ? x : pr[i][c - 1]);
+              else pr[i][c - 1] = (dmode[i] == 1 && dk + c < B) ? x : pr[i][c - 1];
             }
             dmode[i] = 0;
           }
@@ -272,6 +278,7 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
             for (int i = 0; i < RPL; ++i)
               if (ps[i] > j) lrow[i] = div_rn(pr[i][0], ujj);
           }
+          const double s1 = (KIND == kInvert) ? mul_rn(pv[1], rinv) : 0.0;
 #pragma unroll
           for (int i = 0; i < RPL; ++i) {
             const int r = t + PT * i;
@@ -280,14 +287,15 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
             const bool upd = r < n && !is_piv && (KIND == kInvert || below);
             dmode[i] = upd ? 1 : ((KIND == kInvert && is_piv) ? 2 : 0);
             dl[i] = lrow[i];
-            if (upd) {
-              Mm[r * MS + k] = lrow[i];
-              if (KIND == kInvert || k + 1 < B) pr[i][1] = sub_rn(pr[i][1], mul_rn(lrow[i], pv[1]));
-              pr[i][0] = (KIND == kInvert) ? -lrow[i] : lrow[i];
-            }
-            if (KIND == kInvert && is_piv) {
-              pr[i][0] = rinv;
-              pr[i][1] = mul_rn(pr[i][1], rinv);
+            if (upd) Mm[r * MS + k] = lrow[i];
+            const double x1 = sub_rn(pr[i][1], mul_rn(lrow[i], pv[1]));
+            if (KIND == kInvert) {
+              // the pivot row holds pv: its scaled entry is s1 on every lane
+              pr[i][1] = upd ? x1 : (is_piv ? s1 : pr[i][1]);
+              pr[i][0] = upd ? -lrow[i] : (is_piv ? rinv : pr[i][0]);
+            } else {
+              if (k + 1 < B) pr[i][1] = upd ? x1 : pr[i][1];
+              pr[i][0] = upd ? lrow[i] : pr[i][0];
             }
           }
 #pragma unroll
@@ -336,32 +344,81 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
       // ---- 2. the panel's pivot rows at their own step, one thread per column
       for (int c = t; c < P; c += NT) {
         if (!((c < j0 || c >= j0 + B) && (KIND == kInvert || c >= j0 + B))) continue;
-        int q[B];
-        double v[B];
+        if constexpr (!GM) {
+          // Every load is issued before the dependent chains: positions j0 + k < P
+          // hold a valid row even past a short last panel (rows >= n keep their
+          // own position), so the loads need no guard and the steps that panel
+          // does not take only select zeros.
+          int q[B];
+          double v[B];
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
-          q[k] = (k < nb) ? perm[j0 + k] : 0;
-          v[k] = (k < nb) ? M[q[k] * P + (c ^ cta_swz(q[k]))] : 0.0;
-        }
+          for (int k = 0; k < B; ++k) q[k] = perm[j0 + k];
 #pragma unroll
-        for (int k = 1; k < B; ++k)
+          for (int k = 0; k < B; ++k) {
+            const double w = M[q[k] * P + (c ^ cta_swz(q[k]))];
+            v[k] = (k < nb) ? w : 0.0;
+          }
 #pragma unroll
-          for (int k2 = 0; k2 < k; ++k2)
-            if (k < nb) v[k] = sub_rn(v[k], mul_rn(Mm[q[k] * MS + k2], v[k2]));
+          for (int k = 1; k < B; ++k) {
+            double ml[B];
 #pragma unroll
-        for (int k = 0; k < B; ++k) Vs[k * P + c] = v[k];
+            for (int k2 = 0; k2 < k; ++k2) ml[k2] = Mm[q[k] * MS + k2];
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
-          if (k < nb) {
-            double f = v[k];
-            if (KIND == kInvert) {
-              // scaled at its own step, then eliminated by the later pivots
-              f = mul_rn(f, rinv_s[k]);
+            for (int k2 = 0; k2 < k; ++k2)
+              if (k < nb) v[k] = sub_rn(v[k], mul_rn(ml[k2], v[k2]));
+          }
+          double f[B];
+          if (KIND == kInvert) {
+            // scaled at its own step, then eliminated by the later pivots
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+              double mu[B];
+#pragma unroll
+              for (int k2 = k + 1; k2 < B; ++k2) mu[k2] = Mm[q[k] * MS + k2];
+              f[k] = mul_rn(v[k], rinv_s[k]);
 #pragma unroll
               for (int k2 = k + 1; k2 < B; ++k2)
-                if (k2 < nb) f = fma(-Mm[q[k] * MS + k2], v[k2], f);
+                if (k2 < nb) f[k] = fma(-mu[k2], v[k2], f[k]);
             }
-            M[q[k] * P + (c ^ cta_swz(q[k]))] = f;
+          } else {
+#pragma unroll
+            for (int k = 0; k < B; ++k) f[k] = v[k];
+          }
+#pragma unroll
+          for (int k = 0; k < B; ++k) Vs[k * P + c] = v[k];
+#pragma unroll
+          for (int k = 0; k < B; ++k)
+            if (k < nb) M[q[k] * P + (c ^ cta_swz(q[k]))] = f[k];
+        } else {
+          // the workspace classes load from L2 on demand: fewer registers
+          // held across the chains, which their occupancy needs more
+          int q[B];
+          double v[B];
+#pragma unroll
+          for (int k = 0; k < B; ++k) {
+            q[k] = (k < nb) ? perm[j0 + k] : 0;
+            v[k] = (k < nb) ? M[q[k] * P + (c ^ cta_swz(q[k]))] : 0.0;
+          }
+#pragma unroll
+          for (int k = 1; k < B; ++k)
+#pragma unroll
+            for (int k2 = 0; k2 < k; ++k2)
+              if (k < nb) v[k] = sub_rn(v[k], mul_rn(Mm[q[k] * MS + k2], v[k2]));
+#pragma unroll
+          for (int k = 0; k < B; ++k) Vs[k * P + c] = v[k];
+#pragma unroll
+          for (int k = 0; k < B; ++k) {
+            if (k < nb) {
+              double f = v[k];
+              if (KIND == kInvert) {
+                // scaled at its own step, then eliminated by the later pivots
+                f = mul_rn(f, rinv_s[k]);
+#pragma unroll
+                for (int k2 = k + 1; k2 < B; ++k2)
+                  if (k2 < nb) f = fma(-Mm[q[k] * MS + k2], v[k2], f);
+              }
+              M[q[k] * P + (c ^ cta_swz(q[k]))] = f;
+            }
           }
         }
       }
@@ -452,6 +509,23 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
                 for (int u = 0; u < RG; ++u)
 #pragma unroll
                   for (int c = 0; c < CC; ++c) a[u][c] = fma(-mk[u], vk[c], a[u][c]);
+              }
+            } else if (KIND == kInvert && cg < jb) {
+              // a chunk across the panel: its columns left of the panel take the
+              // fused update, column by column as in the shared-memory classes,
+              // so that every class returns the same bits
+#pragma unroll
+              for (int k = 0; k < B; ++k) {
+                double mk[RG], vk[CC];
+#pragma unroll
+                for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
+#pragma unroll
+                for (int c = 0; c < CC; ++c) vk[c] = Vs[k * P + tc + 8 * (cg + c)];
+#pragma unroll
+                for (int u = 0; u < RG; ++u)
+#pragma unroll
+                  for (int c = 0; c < CC; ++c)
+                    a[u][c] = (cg + c < jb) ? fma(-mk[u], vk[c], a[u][c]) : sub_rn(a[u][c], mul_rn(mk[u], vk[c]));
               }
             } else {
 #pragma unroll
