@@ -49,9 +49,9 @@ HBM_FALLBACK_GBS = 6650.0
 # ratio to its algorithmic bytes (captures of a smaller case are scaled by the
 # systems processed): {config: (size class, traffic / algorithmic bytes, capture)}
 TRAFFIC = {
-    1: ("cta64", 438.2 / 487.7, "profiles/cta_exact_kernel_inverse_8192x61.md"),
+    1: ("cta64", 435.6 / 487.7, "profiles/cta_exact_kernel_inverse_8192x61.md"),
     0: ("small28", 25.0 / 25.66, "profiles/small_exact_kernel_solve_4096x27.md"),
-    3: ("cta192", 2294.0 / 248.6, "profiles/cta_exact_kernel_inverse_n161-192_workspace.md"),
+    3: ("cta192", 2242.1 / 248.6, "profiles/cta_exact_kernel_inverse_n161-192_workspace.md"),
     4: ("cta1024", 49803.5 / 373.7, "profiles/cta_exact_kernel_inverse_n897-1024_workspace.md"),
 }
 

@@ -487,7 +487,8 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
 #pragma unroll 1
           for (int cg = 0; cg < CB; cg += CC) {
             // a chunk wholly left of the panel: fused updates for an inverse
-            // (outside GSL's LU), nothing to do for a solve (its L columns)
+            // (outside GSL's LU), nothing to do for a solve (its L columns).
+            // The rule is per chunk, so the candidates of one order share CC.
             const bool left = cg + CC <= jb;
             if (KIND == kSolve && left) continue;
             double a[RG][CC];
@@ -509,23 +510,6 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
                 for (int u = 0; u < RG; ++u)
 #pragma unroll
                   for (int c = 0; c < CC; ++c) a[u][c] = fma(-mk[u], vk[c], a[u][c]);
-              }
-            } else if (KIND == kInvert && cg < jb) {
-              // a chunk across the panel: its columns left of the panel take the
-              // fused update, column by column as in the shared-memory classes,
-              // so that every class returns the same bits
-#pragma unroll
-              for (int k = 0; k < B; ++k) {
-                double mk[RG], vk[CC];
-#pragma unroll
-                for (int u = 0; u < RG; ++u) mk[u] = Mm[row[u] * MS + k];
-#pragma unroll
-                for (int c = 0; c < CC; ++c) vk[c] = Vs[k * P + tc + 8 * (cg + c)];
-#pragma unroll
-                for (int u = 0; u < RG; ++u)
-#pragma unroll
-                  for (int c = 0; c < CC; ++c)
-                    a[u][c] = (cg + c < jb) ? fma(-mk[u], vk[c], a[u][c]) : sub_rn(a[u][c], mul_rn(mk[u], vk[c]));
               }
             } else {
 #pragma unroll

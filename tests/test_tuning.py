@@ -25,3 +25,13 @@ def test_record_matches_table():
         assert tuple(entry["chosen"]) == table[entry["P"]], entry["P"]
         timed = [tuple(c["config"]) for c in entry["candidates"] if "ms" in c]
         assert tuple(entry["chosen"]) in timed
+
+
+def test_candidates_of_one_order_share_storage_and_chunk_width():
+    # an inverse fuses its left-of-panel updates per column in shared memory and
+    # per CC-wide chunk in the workspace: those two choices fix the bits
+    by_p = {}
+    for c in autotune.parse_candidates():
+        by_p.setdefault(c[0], set()).add((c[5], c[3] if c[5] else None))
+    for p, kinds in by_p.items():
+        assert len(kinds) == 1, (p, kinds)
