@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -429,6 +430,16 @@ constexpr size_t kPlanCache = 16;                      // plans cached per threa
 constexpr int64_t kPlanWorkBytes = int64_t(8) << 30;   // workspace the cached plans may hold
 constexpr int64_t kChunkBytes = int64_t(SS_CHUNK_MIB) << 20;
 
+// host pipeline chunk size: SIROCCO_CHUNK_MIB overrides the built-in size (read once)
+static int64_t chunk_bytes() {
+  static const int64_t v = [] {
+    const char* e = std::getenv("SIROCCO_CHUNK_MIB");
+    const long m = e ? std::strtol(e, nullptr, 10) : 0;
+    return (m > 0 && m <= 4096) ? int64_t(m) << 20 : kChunkBytes;
+  }();
+  return v;
+}
+
 struct Context {
   int device = -1;
   cudaStream_t stream = nullptr;
@@ -487,7 +498,7 @@ struct Context {
     while (s0 < nsys) {
       int s1 = s0;
       int64_t bytes = 0;
-      while (s1 < nsys && (s1 == s0 || bytes < kChunkBytes)) {
+      while (s1 < nsys && (s1 == s0 || bytes < chunk_bytes())) {
         bytes += int64_t(n[s1]) * n[s1] * 8;
         ++s1;
       }
@@ -628,7 +639,7 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
   for (int s = 0; s + 1 < nsys && packed; ++s) {
     packed = offA[s + 1] == offA[s] + int64_t(n[s]) * n[s] && (kind != kSolve || offv[s + 1] == offv[s] + n[s]);
   }
-  if (packed && bytesA > size_t(2 * kChunkBytes)) {
+  if (packed && bytesA > size_t(2 * chunk_bytes())) {
     // chunked pipeline: the copies of one chunk overlap the kernels of the others
     Pipeline* pl = nullptr;
     rc = c->get_pipeline(kind, nsys, n, offA, kind == kSolve ? offv : nullptr, md, &pl);
