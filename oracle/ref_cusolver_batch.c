@@ -1,5 +1,5 @@
 /*
- * BASELINE DRIVER -- measurement infrastructure only, never on the engine's path.
+ * Reference-arm helper -- measurement infrastructure only, never on the engine's path.
  *
  * Serial batch loop around the reference's own cuSOLVER build
  * (source/matrix_gpu.cu: gpu_solve_matrix :264-307, gpu_invert_matrix
