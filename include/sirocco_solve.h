@@ -137,6 +137,58 @@ int ion_populations_lockstep(int ncell, int nions, int nelem, const int *elem_fi
                              const int *istate, int h_elem, const double *elem_dens, double *ne, double *den,
                              sirocco_ion_assemble_fn assemble, void *user, int *status, int *iters);
 
+/* The atomic data populate_ion_rate_matrix (source/matrix_ion.c:444-659) reads:
+   the ele[] / ion[] fields it tests, the inner-shell rates with their electron
+   yields (inner_cross[], inner_elec_yield[]) and the charge-exchange entries
+   (charge_exchange[]).  Element e owns ions elem_first[e] .. elem_first[e] +
+   elem_n[e] - 1 in stage order (stage 1 = neutral).  Host arrays. */
+typedef struct sirocco_ion_table {
+  int nions, nelem;
+  const int *elem_z;            /* [nelem] atomic number */
+  const int *elem_first;        /* [nelem] first ion */
+  const int *elem_n;            /* [nelem] ions of the element */
+  const int *elem_istate_max;   /* [nelem] highest stage */
+  const int *ion_istate;        /* [nions] stage */
+  const int *ion_di;            /* [nions] dere_di_flag */
+  const int *ion_dr;            /* [nions] drflag */
+  int n_inner;
+  const int *inner_nion;        /* [n_inner] ion depopulated by inner-shell rate m */
+  const int *inner_yield;       /* [n_inner] its row of yield_prob, -1 without yield data */
+  int n_yield;
+  const double *yield_prob;     /* [n_yield][10] probability of 1..10 ejected electrons */
+  int ncx;
+  const int *cx_nion1;          /* [ncx] ion ionised by charge exchange */
+  const int *cx_nion2;          /* [ncx] its partner; entries count when that is hydrogen */
+} sirocco_ion_table;
+
+/* Per-cell coefficients, cell after cell: pi, rr (pi_rates, rr_rates), di, qr,
+   dr (di_coeffs, qrecomb_coeffs, dr_coeffs) and cxr
+   (charge_exchange_recomb_rates), nions each; cxi
+   (charge_exchange_ioniz_rates), ncx each; inner (inner_rates), n_inner each.
+   Host arrays. */
+typedef struct sirocco_ion_rates {
+  const double *pi, *rr, *di, *qr, *dr, *cxr, *cxi, *inner;
+} sirocco_ion_rates;
+
+/* populate_ion_rate_matrix on the GPU for ncell cells at electron densities
+   ne[c] and neutral / ionised hydrogen densities nh1[c], nh2[c].  The
+   reference's matrix is block-diagonal by element; A receives each cell's
+   element blocks one after another (row-major, elem_n[e]^2 each, elements in
+   order), b each cell's nions right-hand side.  Every entry is bit-identical
+   to the reference's.  Tables whose rates reach outside an element's block (a
+   charge-exchange term above a neutral ion with a nonzero rate, an ionisation
+   or inner-shell yield past the element's last ion) return SIROCCO_EINVAL.
+   Host arrays. */
+int ion_rate_matrices_batched(const sirocco_ion_table *tab, int ncell, const sirocco_ion_rates *rates,
+                              const double *ne, const double *nh1, const double *nh2, double *A, double *b);
+
+/* ion_populations_lockstep with the rate matrices assembled on the GPU from
+   `tab` and `rates` each round (only n_e and the hydrogen densities change
+   between rounds), so no matrix crosses the bus.  Same outputs and rules. */
+int ion_populations_lockstep_rates(const sirocco_ion_table *tab, int ncell, const sirocco_ion_rates *rates,
+                                   int h_elem, const double *elem_dens, double *ne, double *den, int *status,
+                                   int *iters);
+
 /* Macro-atom level populations of one macro element for ncell cells at once:
    the loop of macro_pops (source/macro_gov.c:336-505), one batched solve per
    round over every unfinished cell.  The element has n levels in matrix order

@@ -127,3 +127,110 @@ def cusolver_invert(batch):
     if lib.refgpu_batch_invert(batch.nsys, _p(n), _p(batch.offA), _p(batch.A), _p(out), _p(st)) != 0:
         raise MemoryError("host scratch")
     return out, st
+
+
+# ------------------------------------------------------- ion rate matrices --
+ION_LIB = HERE / "_ref" / "libref_ionmat.so"
+
+
+def ion_rate_matrix(tab, rates, cell: int, xne: float, nh1: float, nh2: float):
+    """Restatement of populate_ion_rate_matrix (source/matrix_ion.c:444-659)
+    for one cell: the full nions x nions matrix and the right-hand side, each
+    entry accumulated block by block in the routine's order (photoionisation,
+    direct ionisation, radiative + three-body recombination, dielectronic
+    recombination, charge-exchange recombination and ionisation, inner-shell
+    ionisation), then each element's first row replaced by ones (:633-655).
+    Python floats round every product and sum separately, as the reference's
+    x86-64 build does.  `tab` and `rates` follow python_b200.workloads.IonTable
+    / IonRates."""
+    n = tab.nions
+    elem_of = tab.elem_of()
+    z = [int(tab.elem_z[elem_of[i]]) for i in range(n)]
+    first = [int(tab.elem_first[elem_of[i]]) for i in range(n)]
+    imax = [int(tab.elem_istate_max[elem_of[i]]) for i in range(n)]
+    ist = [int(v) for v in tab.ion_istate]
+    pi, rr = [float(v) for v in rates.pi[cell]], [float(v) for v in rates.rr[cell]]
+    di, qr, dr = [float(v) for v in rates.di[cell]], [float(v) for v in rates.qr[cell]], [float(v) for v in rates.dr[cell]]
+    cxr = [float(v) for v in rates.cxr[cell]]
+    cxi = [float(v) for v in rates.cxi[cell]]
+    inner = [float(v) for v in rates.inner[cell]]
+    m = [[0.0] * n for _ in range(n)]
+    for mm in range(n):                                   # PI depopulates (:477-483)
+        if ist[mm] != imax[mm]:
+            m[mm][mm] -= pi[mm]
+    for nn in range(n - 1):                               # PI populates (:487-497)
+        if ist[nn] != imax[nn] and z[nn + 1] == z[nn]:
+            m[nn + 1][nn] += pi[nn]
+    for mm in range(n):                                   # DI depopulates (:501-507)
+        if ist[mm] != imax[mm] and tab.ion_di[mm] > 0:
+            m[mm][mm] -= xne * di[mm]
+    for nn in range(n - 1):                               # DI populates (:511-520)
+        if ist[nn] != imax[nn] and z[nn + 1] == z[nn] and tab.ion_di[nn] > 0:
+            m[nn + 1][nn] += xne * di[nn]
+    for mm in range(n):                                   # RR depopulates (:525-531)
+        if mm != first[mm]:
+            m[mm][mm] -= xne * (rr[mm] + xne * qr[mm])
+    for nn in range(1, n):                                # RR populates (:535-544)
+        if nn != first[nn] and z[nn - 1] == z[nn]:
+            m[nn - 1][nn] += xne * (rr[nn] + xne * qr[nn])
+    for mm in range(n):                                   # DR depopulates (:548-554)
+        if mm != first[mm] and tab.ion_dr[mm] > 0:
+            m[mm][mm] -= xne * dr[mm]
+    for nn in range(1, n):                                # DR populates, flag of the lower ion (:562-572)
+        if nn != first[nn] and z[nn - 1] == z[nn] and tab.ion_dr[nn - 1] > 0:
+            m[nn - 1][nn] += xne * dr[nn]
+    if tab.ncx > 0:                                       # charge-exchange recombination (:576-586)
+        for mm in range(n):
+            if z[mm] != 1 and ist[mm] != 0:
+                m[mm][mm] -= cxr[mm] * nh1
+                m[mm - 1][mm] += cxr[mm] * nh1
+    for k in range(tab.ncx):                              # charge-exchange ionisation (:590-596)
+        if z[int(tab.cx_nion2[k])] == 1:
+            o = int(tab.cx_nion1[k])
+            m[o][o] -= cxi[k] * nh2
+            m[o + 1][o] += cxi[k] * nh2
+    for k in range(tab.n_inner):                          # inner-shell ionisation (:599-613)
+        y = int(tab.inner_yield[k])
+        if y != -1:
+            o = int(tab.inner_nion[k])
+            m[o][o] -= inner[k]
+            ne_ = min(z[o] - ist[o] + 1, 11)
+            for d in range(1, ne_):
+                m[o + d][o] += inner[k] * float(tab.yield_prob[y][d - 1])
+    b = [0.0] * n
+    for nn in range(n):                                   # first row of each element (:633-655)
+        if nn == first[nn]:
+            b[nn] = 1.0
+            for mm in range(n):
+                m[nn][mm] = 1.0 if z[mm] == z[nn] else 0.0
+    return np.array(m, dtype=np.float64), np.array(b, dtype=np.float64)
+
+
+def ion_reference_available() -> bool:
+    return ION_LIB.exists()
+
+
+def ref_ion_rate_matrix(tab, rates, cell: int, xne: float, nh1: float, nh2: float):
+    """The reference's own populate_ion_rate_matrix (oracle/_ref/libref_ionmat.so)
+    on the same inputs: (A, b, return value)."""
+    lib = ctypes.CDLL(str(ION_LIB))
+    f = lib.refion_assemble
+    f.restype = c_int
+    n = tab.nions
+    A = np.zeros((n, n), dtype=np.float64)
+    b = np.zeros(n, dtype=np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    elem_of = i32(tab.elem_of())
+    args = [i32(tab.elem_z), i32(tab.elem_first), i32(tab.elem_istate_max), elem_of, i32(tab.ion_istate),
+            i32(tab.ion_di), i32(tab.ion_dr)]
+    inner_nion, inner_yield = i32(tab.inner_nion), i32(tab.inner_yield)
+    yp = f64(tab.yield_prob).reshape(-1)
+    cx1, cx2 = i32(tab.cx_nion1), i32(tab.cx_nion2)
+    cells = [f64(getattr(rates, k)[cell]) for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")]
+    keep = args + [inner_nion, inner_yield, yp, cx1, cx2] + cells + [A, b]
+    rc = f(c_int(n), c_int(tab.nelem), *[_p(a) for a in args], c_int(tab.n_inner), _p(inner_nion), _p(inner_yield),
+           c_int(len(tab.yield_prob)), _p(yp), c_int(tab.ncx), _p(cx1), _p(cx2), *[_p(a) for a in cells],
+           ctypes.c_double(xne), ctypes.c_double(nh1), ctypes.c_double(nh2), _p(A), _p(b))
+    del keep
+    return A, b, rc

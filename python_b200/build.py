@@ -48,6 +48,8 @@ def build_oracle(reference: bool = True) -> None:
     ref_tree = Path(os.environ.get("SIROCCO_REFERENCE", "/root/reference"))
     if reference and (ref_tree / "source" / "matrix_cpu.c").exists():
         targets.append("ref")
+        if (ref_tree / "source" / "matrix_ion.c").exists():
+            targets.append("refion")
         if (ref_tree / "source" / "matrix_gpu.cu").exists():
             targets.append("refgpu")
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), f"REF={ref_tree}", *targets], check=True)

@@ -19,12 +19,14 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <functional>
 #include <unordered_map>
 #include <vector>
 
 #include "../../include/sirocco_solve.h"
 #include "kernels_cta.cuh"
 #include "kernels_global.cuh"
+#include "kernels_ionasm.cuh"
 #include "kernels_matom.cuh"
 #include "kernels_mixed.cuh"
 #include "kernels_small.cuh"
@@ -451,6 +453,7 @@ struct Context {
   std::vector<uint64_t> pipe_order;
   DevBuf bA, bb, bx, bst;
   DevBuf bR, bC, bOv, bN, bOa, bQs, bQl, bQz, bQt;   // macro-atom epilogue and draws
+  DevBuf bIT, bI64, bID, bIL, bIS, bIA, bIB, bIX, bISt;   // ion rate-matrix assembly
   int mode = SIROCCO_FP64;
   ~Context() { release(); }
   void release() {
@@ -798,17 +801,11 @@ constexpr double kDensityMin = 1.0e-20;   // atomic.h:9
 constexpr double kFracError = 0.03;       // python.h:1212
 constexpr int kMaxIterations = 200;       // python.h:1211
 
-static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_first, const int* elem_n,
-                            const int* istate, int h_elem, const double* elem_dens, double* ne, double* den,
-                            sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
-  if (ncell == 0) return 0;
-  if (ncell < 0 || nions < 1 || nelem < 1 || !elem_first || !elem_n || !istate || !elem_dens || !ne || !den ||
-      !assemble || !status || !iters || h_elem >= nelem) {
-    set_error("invalid lock-step arguments");
-    return SIROCCO_EINVAL;
-  }
-  std::vector<int> elem_of(nions, -1);
-  int64_t blkA = 0;
+// Elements own consecutive ion ranges that together cover every ion once.
+static int check_ion_elements(int nions, int nelem, const int* elem_first, const int* elem_n, std::vector<int>& elem_of,
+                              int64_t& blkA) {
+  elem_of.assign(nions, -1);
+  blkA = 0;
   for (int e = 0; e < nelem; ++e) {
     if (elem_n[e] < 1 || elem_first[e] < 0 || elem_first[e] + elem_n[e] > nions) {
       set_error("element %d: ions [%d, %d) outside 0..%d", e, elem_first[e], elem_first[e] + elem_n[e], nions);
@@ -828,6 +825,20 @@ static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_fir
       set_error("ion %d belongs to no element", i);
       return SIROCCO_EINVAL;
     }
+  return 0;
+}
+
+// One round of the lock-step for the listed cells: assemble and solve their
+// element systems; x receives nions populations per cell (element order), st
+// the solve codes of the cell's nelem blocks.
+using IonRoundFn = std::function<int(int na, const int* cells, const double* ne, const double* nh1, const double* nh2,
+                                     double* x, int* st)>;
+
+// The n_e iteration of matrix_ion_populations (source/matrix_ion.c:219-382)
+// over many cells at once: each round solves every unfinished cell.
+static int ion_lockstep_core(int ncell, int nions, int nelem, const int* elem_first, const int* elem_n,
+                             const int* istate, int h_elem, const double* elem_dens, const std::vector<int>& elem_of,
+                             double* ne, double* den, const IonRoundFn& round, int* status, int* iters) {
   std::vector<double> xne(ne, ne + ncell), cur(den, den + size_t(ncell) * nions);
   std::vector<int> active(ncell);
   for (int c = 0; c < ncell; ++c) {
@@ -835,9 +846,8 @@ static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_fir
     status[c] = -2;
     iters[c] = 0;
   }
-  std::vector<double> A, b, x, nh1, nh2, nea;
-  std::vector<int> n, st;
-  std::vector<int64_t> offA, offv;
+  std::vector<double> x, nh1, nh2, nea;
+  std::vector<int> st;
   for (int it = 0; it < kMaxIterations && !active.empty(); ++it) {
     const int na = int(active.size());
     nea.resize(na);
@@ -857,30 +867,9 @@ static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_fir
         }
       }
     }
-    A.assign(size_t(na) * blkA, 0.0);
-    b.assign(size_t(na) * nions, 0.0);
-    const int arc = assemble(user, na, active.data(), nea.data(), nh1.data(), nh2.data(), A.data(), b.data());
-    if (arc != 0) {
-      set_error("assembly callback returned %d", arc);
-      return SIROCCO_EINVAL;
-    }
-    const int nsys = na * nelem;
-    n.resize(nsys);
-    offA.resize(nsys);
-    offv.resize(nsys);
-    st.assign(nsys, 0);
     x.assign(size_t(na) * nions, 0.0);
-    for (int i = 0, s = 0; i < na; ++i) {
-      int64_t oa = int64_t(i) * blkA;
-      for (int e = 0; e < nelem; ++e, ++s) {
-        n[s] = elem_n[e];
-        offA[s] = oa;
-        offv[s] = int64_t(i) * nions + elem_first[e];
-        oa += int64_t(elem_n[e]) * elem_n[e];
-      }
-    }
-    int rc = run_batched(kSolve, nsys, n.data(), offA.data(), A.data(), offv.data(), b.data(), x.data(), st.data(),
-                         ctx()->mode);
+    st.assign(size_t(na) * nelem, 0);
+    int rc = round(na, active.data(), nea.data(), nh1.data(), nh2.data(), x.data(), st.data());
     if (rc) return rc;
     std::vector<int> next;
     for (int i = 0; i < na; ++i) {
@@ -912,6 +901,291 @@ static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_fir
   }
   // cells still active ran out of iterations (matrix_ion.c:366-382): status -2, inputs kept
   return 0;
+}
+
+// The batched layout of na cells' element systems: cell i's blocks one after
+// another (element order), its right-hand side and solution at i * nions.
+static void ion_block_layout(int na, int nions, int nelem, const int* elem_first, const int* elem_n, int64_t blkA,
+                             std::vector<int>& n, std::vector<int64_t>& offA, std::vector<int64_t>& offv) {
+  const int nsys = na * nelem;
+  n.resize(nsys);
+  offA.resize(nsys);
+  offv.resize(nsys);
+  for (int i = 0, s = 0; i < na; ++i) {
+    int64_t oa = int64_t(i) * blkA;
+    for (int e = 0; e < nelem; ++e, ++s) {
+      n[s] = elem_n[e];
+      offA[s] = oa;
+      offv[s] = int64_t(i) * nions + elem_first[e];
+      oa += int64_t(elem_n[e]) * elem_n[e];
+    }
+  }
+}
+
+static int run_ion_lockstep(int ncell, int nions, int nelem, const int* elem_first, const int* elem_n,
+                            const int* istate, int h_elem, const double* elem_dens, double* ne, double* den,
+                            sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
+  if (ncell == 0) return 0;
+  if (ncell < 0 || nions < 1 || nelem < 1 || !elem_first || !elem_n || !istate || !elem_dens || !ne || !den ||
+      !assemble || !status || !iters || h_elem >= nelem) {
+    set_error("invalid lock-step arguments");
+    return SIROCCO_EINVAL;
+  }
+  std::vector<int> elem_of;
+  int64_t blkA = 0;
+  int rc = check_ion_elements(nions, nelem, elem_first, elem_n, elem_of, blkA);
+  if (rc) return rc;
+  std::vector<double> A, b;
+  std::vector<int> n;
+  std::vector<int64_t> offA, offv;
+  auto round = [&](int na, const int* cells, const double* nea, const double* nh1, const double* nh2, double* x,
+                   int* st) -> int {
+    A.assign(size_t(na) * blkA, 0.0);
+    b.assign(size_t(na) * nions, 0.0);
+    const int arc = assemble(user, na, cells, nea, nh1, nh2, A.data(), b.data());
+    if (arc != 0) {
+      set_error("assembly callback returned %d", arc);
+      return SIROCCO_EINVAL;
+    }
+    ion_block_layout(na, nions, nelem, elem_first, elem_n, blkA, n, offA, offv);
+    return run_batched(kSolve, na * nelem, n.data(), offA.data(), A.data(), offv.data(), b.data(), x, st,
+                       ctx()->mode);
+  };
+  return ion_lockstep_core(ncell, nions, nelem, elem_first, elem_n, istate, h_elem, elem_dens, elem_of, ne, den,
+                           round, status, iters);
+}
+
+// ------------------------------------------------- ion rate-matrix assembly --
+// Checks a table and its rates, builds the per-ion flags and the per-ion
+// lists of charge-exchange and inner-shell entries, and uploads everything for
+// ion_assemble_kernel.  v gets the device pointers of everything but the
+// per-round arrays.
+static int ion_asm_prepare(const sirocco_ion_table* t, int ncell, const sirocco_ion_rates* r, Context* c,
+                           IonAsmView& v, std::vector<int>& elem_of, int64_t& blkA) {
+  if (!t || !r || t->nions < 1 || t->nelem < 1 || !t->elem_z || !t->elem_first || !t->elem_n || !t->elem_istate_max ||
+      !t->ion_istate || !t->ion_di || !t->ion_dr || t->n_inner < 0 || t->n_yield < 0 || t->ncx < 0 ||
+      (t->n_inner > 0 && (!t->inner_nion || !t->inner_yield)) || (t->n_yield > 0 && !t->yield_prob) ||
+      (t->ncx > 0 && (!t->cx_nion1 || !t->cx_nion2)) || !r->pi || !r->rr || !r->di || !r->qr || !r->dr || !r->cxr ||
+      (t->ncx > 0 && !r->cxi) || (t->n_inner > 0 && !r->inner)) {
+    set_error("invalid ion table or rates");
+    return SIROCCO_EINVAL;
+  }
+  const int nions = t->nions, nelem = t->nelem;
+  int rc = check_ion_elements(nions, nelem, t->elem_first, t->elem_n, elem_of, blkA);
+  if (rc) return rc;
+  auto last_of = [&](int i) { const int e = elem_of[i]; return t->elem_first[e] + t->elem_n[e] - 1; };
+  std::vector<int> flags(nions), zion(nions);
+  for (int i = 0; i < nions; ++i) {
+    const int e = elem_of[i];
+    zion[i] = t->elem_z[e];
+    flags[i] = (t->ion_istate[i] == t->elem_istate_max[e] ? 1 : 0) | (t->ion_di[i] > 0 ? 2 : 0) |
+               (t->ion_dr[i] > 0 ? 4 : 0);
+  }
+  // charge-exchange ionisation against hydrogen, per ionised ion, in entry order
+  std::vector<int> cx_start(nions + 1, 0), in_start(nions + 1, 0), cx_idx, in_idx, in_yield;
+  std::vector<std::vector<int>> cx_of(nions), in_of(nions);
+  for (int m = 0; m < t->ncx; ++m) {
+    const int o = t->cx_nion1[m], p = t->cx_nion2[m];
+    if (o < 0 || o >= nions || p < 0 || p >= nions) {
+      set_error("charge-exchange entry %d: ions %d, %d outside 0..%d", m, o, p, nions);
+      return SIROCCO_EINVAL;
+    }
+    if (zion[p] != 1) continue;
+    if (o + 1 > last_of(o)) {
+      set_error("charge-exchange entry %d ionises ion %d, the last of its element", m, o);
+      return SIROCCO_EINVAL;
+    }
+    cx_of[o].push_back(m);
+  }
+  for (int m = 0; m < t->n_inner; ++m) {
+    const int o = t->inner_nion[m], y = t->inner_yield[m];
+    if (o < 0 || o >= nions || y < -1 || y >= t->n_yield) {
+      set_error("inner-shell rate %d: ion %d or yield row %d out of range", m, o, y);
+      return SIROCCO_EINVAL;
+    }
+    if (y == -1) continue;
+    const int nel = std::min(zion[o] - t->ion_istate[o] + 1, 11);
+    if (nel > 1 && o + nel - 1 > last_of(o)) {
+      set_error("inner-shell rate %d of ion %d yields past its element's last ion", m, o);
+      return SIROCCO_EINVAL;
+    }
+    in_of[o].push_back(m);
+  }
+  for (int i = 0; i < nions; ++i) {
+    cx_start[i + 1] = cx_start[i] + int(cx_of[i].size());
+    cx_idx.insert(cx_idx.end(), cx_of[i].begin(), cx_of[i].end());
+    in_start[i + 1] = in_start[i] + int(in_of[i].size());
+    for (int m : in_of[i]) {
+      in_idx.push_back(m);
+      in_yield.push_back(t->inner_yield[m]);
+    }
+  }
+  // charge-exchange recombination writes above each ion (matrix_ion.c:579-585);
+  // above a neutral ion that entry belongs to another element and must be zero
+  if (t->ncx > 0)
+    for (int e = 0; e < nelem; ++e) {
+      if (t->elem_z[e] == 1) continue;
+      const int f = t->elem_first[e];
+      for (int cc = 0; cc < ncell; ++cc)
+        if (r->cxr[size_t(cc) * nions + f] != 0.0) {
+          set_error("cell %d: charge-exchange recombination of neutral ion %d reaches outside its element", cc, f);
+          return SIROCCO_EINVAL;
+        }
+    }
+  // ints: elem_first, elem_n, ion_z, ion_istate, flags, cx_start, cx_idx, in_start, in_idx, in_yield
+  std::vector<int> ints;
+  std::vector<size_t> io;
+  auto put_i = [&](const int* p, size_t k) { io.push_back(ints.size()); ints.insert(ints.end(), p, p + k); };
+  put_i(t->elem_first, nelem);
+  put_i(t->elem_n, nelem);
+  put_i(zion.data(), nions);
+  put_i(t->ion_istate, nions);
+  put_i(flags.data(), nions);
+  put_i(cx_start.data(), nions + 1);
+  put_i(cx_idx.data(), cx_idx.size());
+  put_i(in_start.data(), nions + 1);
+  put_i(in_idx.data(), in_idx.size());
+  put_i(in_yield.data(), in_yield.size());
+  std::vector<int64_t> boff(nelem);
+  for (int e = 0, o = 0; e < nelem; ++e) {
+    boff[e] = o;
+    o += t->elem_n[e] * t->elem_n[e];
+  }
+  const size_t cn = size_t(ncell) * nions;
+  std::vector<size_t> dsz = {size_t(t->n_yield) * 10, cn, cn, cn, cn, cn, cn, size_t(ncell) * t->ncx,
+                             size_t(ncell) * t->n_inner};
+  const double* dsrc[] = {t->yield_prob, r->pi, r->rr, r->di, r->qr, r->dr, r->cxr, r->cxi, r->inner};
+  size_t dtot = 0;
+  for (size_t k : dsz) dtot += k;
+  if ((rc = c->bIT.ensure(sizeof(int) * std::max<size_t>(ints.size(), 1))) ||
+      (rc = c->bI64.ensure(sizeof(int64_t) * nelem)) || (rc = c->bID.ensure(sizeof(double) * std::max<size_t>(dtot, 1))))
+    return rc;
+  int* di_ = static_cast<int*>(c->bIT.ptr);
+  double* dd = static_cast<double*>(c->bID.ptr);
+  SS_CUDA(cudaMemcpy(di_, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice));
+  SS_CUDA(cudaMemcpy(c->bI64.ptr, boff.data(), sizeof(int64_t) * nelem, cudaMemcpyHostToDevice));
+  const double* dptr[9];
+  size_t off = 0;
+  for (int k = 0; k < 9; ++k) {
+    dptr[k] = dd + off;
+    if (dsz[k] > 0) SS_CUDA(cudaMemcpy(dd + off, dsrc[k], sizeof(double) * dsz[k], cudaMemcpyHostToDevice));
+    off += dsz[k];
+  }
+  v = IonAsmView{};
+  v.nions = nions;
+  v.nelem = nelem;
+  v.ncx = t->ncx;
+  v.n_inner = t->n_inner;
+  v.elem_first = di_ + io[0];
+  v.elem_n = di_ + io[1];
+  v.ion_z = di_ + io[2];
+  v.ion_istate = di_ + io[3];
+  v.ion_flags = di_ + io[4];
+  v.cx_start = di_ + io[5];
+  v.cx_idx = di_ + io[6];
+  v.in_start = di_ + io[7];
+  v.in_idx = di_ + io[8];
+  v.in_yield = di_ + io[9];
+  v.blk_off = static_cast<const int64_t*>(c->bI64.ptr);
+  v.blk_cell = blkA;
+  v.yield = dptr[0];
+  v.pi = dptr[1];
+  v.rr = dptr[2];
+  v.di = dptr[3];
+  v.qr = dptr[4];
+  v.dr = dptr[5];
+  v.cxr = dptr[6];
+  v.cxi = dptr[7];
+  v.inner = dptr[8];
+  return 0;
+}
+
+// Assembles the listed cells' element systems into the context's device
+// buffers bIA (A) and bIB (b) on the context stream.
+static int ion_asm_round(Context* c, IonAsmView& v, int na, const int* cells, const double* ne, const double* nh1,
+                         const double* nh2) {
+  int rc;
+  if ((rc = c->bIL.ensure(sizeof(int) * size_t(na))) || (rc = c->bIS.ensure(sizeof(double) * 3 * size_t(na))) ||
+      (rc = c->bIA.ensure(sizeof(double) * size_t(na) * size_t(v.blk_cell))) ||
+      (rc = c->bIB.ensure(sizeof(double) * size_t(na) * size_t(v.nions))))
+    return rc;
+  double* ds = static_cast<double*>(c->bIS.ptr);
+  SS_CUDA(cudaMemcpyAsync(c->bIL.ptr, cells, sizeof(int) * size_t(na), cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(ds, ne, sizeof(double) * size_t(na), cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(ds + na, nh1, sizeof(double) * size_t(na), cudaMemcpyHostToDevice, c->stream));
+  SS_CUDA(cudaMemcpyAsync(ds + 2 * size_t(na), nh2, sizeof(double) * size_t(na), cudaMemcpyHostToDevice, c->stream));
+  v.count = na;
+  v.cells = static_cast<const int*>(c->bIL.ptr);
+  v.ne = ds;
+  v.nh1 = ds + na;
+  v.nh2 = ds + 2 * size_t(na);
+  v.A = static_cast<double*>(c->bIA.ptr);
+  v.b = static_cast<double*>(c->bIB.ptr);
+  const int64_t warps = int64_t(na) * v.nelem;
+  const int64_t grid = (warps * 32 + kIonAsmThreads - 1) / kIonAsmThreads;
+  ion_assemble_kernel<<<unsigned(grid), kIonAsmThreads, 0, c->stream>>>(v);
+  SS_CUDA(cudaGetLastError());
+  return 0;
+}
+
+static int run_ion_rate_matrices(const sirocco_ion_table* t, int ncell, const sirocco_ion_rates* r, const double* ne,
+                                 const double* nh1, const double* nh2, double* A, double* b) {
+  if (ncell == 0) return 0;
+  if (ncell < 0 || !ne || !nh1 || !nh2 || !A || !b) {
+    set_error("invalid rate-matrix arguments");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  IonAsmView v;
+  std::vector<int> elem_of;
+  int64_t blkA = 0;
+  if ((rc = ion_asm_prepare(t, ncell, r, c, v, elem_of, blkA))) return rc;
+  std::vector<int> cells(ncell);
+  for (int i = 0; i < ncell; ++i) cells[i] = i;
+  if ((rc = ion_asm_round(c, v, ncell, cells.data(), ne, nh1, nh2))) return rc;
+  SS_CUDA(cudaMemcpyAsync(A, v.A, sizeof(double) * size_t(ncell) * size_t(blkA), cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaMemcpyAsync(b, v.b, sizeof(double) * size_t(ncell) * size_t(t->nions), cudaMemcpyDeviceToHost,
+                          c->stream));
+  SS_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+static int run_ion_lockstep_rates(const sirocco_ion_table* t, int ncell, const sirocco_ion_rates* r, int h_elem,
+                                  const double* elem_dens, double* ne, double* den, int* status, int* iters) {
+  if (ncell == 0) return 0;
+  if (ncell < 0 || !t || !elem_dens || !ne || !den || !status || !iters || h_elem >= t->nelem) {
+    set_error("invalid lock-step arguments");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  IonAsmView v;
+  std::vector<int> elem_of;
+  int64_t blkA = 0;
+  if ((rc = ion_asm_prepare(t, ncell, r, c, v, elem_of, blkA))) return rc;
+  const int nions = t->nions, nelem = t->nelem;
+  std::vector<int> n;
+  std::vector<int64_t> offA, offv;
+  auto round = [&](int na, const int* cells, const double* nea, const double* nh1, const double* nh2, double* x,
+                   int* st) -> int {
+    int rc2 = ion_asm_round(c, v, na, cells, nea, nh1, nh2);
+    if (rc2) return rc2;
+    if ((rc2 = c->bIX.ensure(sizeof(double) * size_t(na) * nions)) ||
+        (rc2 = c->bISt.ensure(sizeof(int) * size_t(na) * nelem)))
+      return rc2;
+    ion_block_layout(na, nions, nelem, t->elem_first, t->elem_n, blkA, n, offA, offv);
+    rc2 = run_batched(kSolve, na * nelem, n.data(), offA.data(), v.A, offv.data(), v.b,
+                      static_cast<double*>(c->bIX.ptr), static_cast<int*>(c->bISt.ptr), c->mode);
+    if (rc2) return rc2;
+    SS_CUDA(cudaMemcpy(x, c->bIX.ptr, sizeof(double) * size_t(na) * nions, cudaMemcpyDeviceToHost));
+    SS_CUDA(cudaMemcpy(st, c->bISt.ptr, sizeof(int) * size_t(na) * nelem, cudaMemcpyDeviceToHost));
+    return 0;
+  };
+  return ion_lockstep_core(ncell, nions, nelem, t->elem_first, t->elem_n, t->ion_istate, h_elem, elem_dens, elem_of,
+                           ne, den, round, status, iters);
 }
 
 // --------------------------------------------------------- macro-atom pops --
@@ -1214,6 +1488,16 @@ int ion_populations_lockstep(int ncell, int nions, int nelem, const int* elem_fi
                              sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
   return ss::run_ion_lockstep(ncell, nions, nelem, elem_first, elem_n, istate, h_elem, elem_dens, ne, den, assemble,
                               user, status, iters);
+}
+
+int ion_rate_matrices_batched(const sirocco_ion_table* tab, int ncell, const sirocco_ion_rates* rates, const double* ne,
+                              const double* nh1, const double* nh2, double* A, double* b) {
+  return ss::run_ion_rate_matrices(tab, ncell, rates, ne, nh1, nh2, A, b);
+}
+
+int ion_populations_lockstep_rates(const sirocco_ion_table* tab, int ncell, const sirocco_ion_rates* rates, int h_elem,
+                                   const double* elem_dens, double* ne, double* den, int* status, int* iters) {
+  return ss::run_ion_lockstep_rates(tab, ncell, rates, h_elem, elem_dens, ne, den, status, iters);
 }
 
 int macro_pops_lockstep(int ncell, int n, int nion, const int* ion_first, const int* ion_nlte, const double* g,

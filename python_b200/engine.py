@@ -30,6 +30,7 @@ EXPORTS = (
     "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
     "sirocco_plan_destroy", "sirocco_last_error", "solve_matrix_batched_noalloc",
     "matom_matrices_batched", "matom_sample_batched", "ion_populations_lockstep", "macro_pops_lockstep",
+    "ion_rate_matrices_batched", "ion_populations_lockstep_rates",
 )
 
 _lib = None
@@ -38,6 +39,20 @@ _lib = None
 MACRO_ASSEMBLE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_int, POINTER(c_int), POINTER(c_int), POINTER(c_double))
 ASSEMBLE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_double),
                                POINTER(c_double), POINTER(c_double), POINTER(c_double))
+
+
+class IonTableC(ctypes.Structure):
+    """sirocco_ion_table (include/sirocco_solve.h)."""
+    _fields_ = [("nions", c_int), ("nelem", c_int), ("elem_z", c_void_p), ("elem_first", c_void_p),
+                ("elem_n", c_void_p), ("elem_istate_max", c_void_p), ("ion_istate", c_void_p), ("ion_di", c_void_p),
+                ("ion_dr", c_void_p), ("n_inner", c_int), ("inner_nion", c_void_p), ("inner_yield", c_void_p),
+                ("n_yield", c_int), ("yield_prob", c_void_p), ("ncx", c_int), ("cx_nion1", c_void_p),
+                ("cx_nion2", c_void_p)]
+
+
+class IonRatesC(ctypes.Structure):
+    """sirocco_ion_rates (include/sirocco_solve.h)."""
+    _fields_ = [(k, c_void_p) for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")]
 
 
 class EngineError(RuntimeError):
@@ -90,6 +105,11 @@ def load() -> ctypes.CDLL:
     lib.ion_populations_lockstep.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                                              c_void_p, c_void_p, ASSEMBLE_FN, c_void_p, c_void_p, c_void_p]
     lib.ion_populations_lockstep.restype = c_int
+    lib.ion_rate_matrices_batched.argtypes = [POINTER(IonTableC), c_int, POINTER(IonRatesC)] + [c_void_p] * 5
+    lib.ion_rate_matrices_batched.restype = c_int
+    lib.ion_populations_lockstep_rates.argtypes = [POINTER(IonTableC), c_int, POINTER(IonRatesC), c_int] + \
+        [c_void_p] * 5
+    lib.ion_populations_lockstep_rates.restype = c_int
     lib.macro_pops_lockstep.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                         MACRO_ASSEMBLE_FN, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.macro_pops_lockstep.restype = c_int
@@ -242,6 +262,59 @@ def ion_populations_lockstep(elem_first, elem_n, istate, h_elem: int, elem_dens:
     rc = lib.ion_populations_lockstep(ncell, nions, elem_n.size, _ptr(elem_first), _ptr(elem_n), _ptr(istate), h_elem,
                                       _ptr(elem_dens), _ptr(ne), _ptr(den), fn, None, _ptr(status), _ptr(iters))
     _check(rc, "ion_populations_lockstep")
+    return status, iters
+
+
+def _ion_c(tab, rates):
+    """The C views of a workloads.IonTable / IonRates and the arrays they point into."""
+    i32 = lambda a: np.ascontiguousarray(a, np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, np.float64)
+    keep = dict(elem_z=i32(tab.elem_z), elem_first=i32(tab.elem_first), elem_n=i32(tab.elem_n),
+                elem_istate_max=i32(tab.elem_istate_max), ion_istate=i32(tab.ion_istate), ion_di=i32(tab.ion_di),
+                ion_dr=i32(tab.ion_dr), inner_nion=i32(tab.inner_nion), inner_yield=i32(tab.inner_yield),
+                yield_prob=f64(tab.yield_prob).reshape(-1), cx_nion1=i32(tab.cx_nion1), cx_nion2=i32(tab.cx_nion2))
+    t = IonTableC(tab.nions, tab.nelem, *[keep[k].ctypes.data for k in (
+        "elem_z", "elem_first", "elem_n", "elem_istate_max", "ion_istate", "ion_di", "ion_dr")],
+        tab.n_inner, keep["inner_nion"].ctypes.data, keep["inner_yield"].ctypes.data, len(tab.yield_prob),
+        keep["yield_prob"].ctypes.data, tab.ncx, keep["cx_nion1"].ctypes.data, keep["cx_nion2"].ctypes.data)
+    rk = {k: f64(getattr(rates, k)) for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")}
+    r = IonRatesC(*[rk[k].ctypes.data for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")])
+    return t, r, (keep, rk)
+
+
+def ion_rate_matrices(tab, rates, ne, nh1, nh2):
+    """populate_ion_rate_matrix on the GPU for every cell of ``rates``
+    (ion_rate_matrices_batched): returns (A, b), A the cells' element blocks
+    packed cell after cell, b [ncell, nions]."""
+    lib = load()
+    t, r, keep = _ion_c(tab, rates)
+    ncell = rates.ncell
+    blk = int((np.asarray(tab.elem_n, np.int64) ** 2).sum())
+    ne, nh1, nh2 = (np.ascontiguousarray(a, np.float64) for a in (ne, nh1, nh2))
+    A = np.empty(ncell * blk, np.float64)
+    b = np.empty((ncell, tab.nions), np.float64)
+    rc = lib.ion_rate_matrices_batched(ctypes.byref(t), ncell, ctypes.byref(r), _ptr(ne), _ptr(nh1), _ptr(nh2),
+                                       _ptr(A), _ptr(b))
+    _check(rc, "ion_rate_matrices_batched")
+    del keep
+    return A, b
+
+
+def ion_populations_lockstep_rates(tab, rates, h_elem: int, elem_dens: np.ndarray, ne: np.ndarray, den: np.ndarray):
+    """ion_populations_lockstep with the rate matrices assembled on the GPU
+    (ion_populations_lockstep_rates).  ``ne`` and ``den`` are updated in place
+    for the cells that converge; returns (status, iters)."""
+    lib = load()
+    t, r, keep = _ion_c(tab, rates)
+    elem_dens = np.ascontiguousarray(elem_dens, np.float64)
+    assert ne.dtype == np.float64 and ne.flags.c_contiguous and den.dtype == np.float64 and den.flags.c_contiguous
+    ncell = den.shape[0]
+    status = np.full(ncell, -99, np.int32)
+    iters = np.zeros(ncell, np.int32)
+    rc = lib.ion_populations_lockstep_rates(ctypes.byref(t), ncell, ctypes.byref(r), h_elem, _ptr(elem_dens),
+                                            _ptr(ne), _ptr(den), _ptr(status), _ptr(iters))
+    _check(rc, "ion_populations_lockstep_rates")
+    del keep
     return status, iters
 
 

@@ -262,3 +262,123 @@ def dense_batch(kind, sizes, seed, log_spread=0.0) -> Batch:
 def from_matrices(kind, mats, rhs=None) -> Batch:
     return _pack(kind, [np.ascontiguousarray(m, dtype=np.float64) for m in mats],
                  [np.ascontiguousarray(r, dtype=np.float64) for r in rhs] if rhs is not None else None)
+
+
+# ------------------------------------------------ ion tables and rate sets --
+@dataclass
+class IonTable:
+    """The atomic-data part of an ion rate matrix (source/atomic.h ele[] / ion[] /
+    inner_cross[] / charge_exchange[] as populate_ion_rate_matrix reads them).
+    Elements hold consecutive ions in stage order; ion stage 1 is neutral."""
+    elem_z: np.ndarray            # [nelem] atomic number
+    elem_first: np.ndarray        # [nelem] first ion of the element
+    elem_n: np.ndarray            # [nelem] ions of the element
+    elem_istate_max: np.ndarray   # [nelem] highest stage
+    ion_istate: np.ndarray        # [nions] stage
+    ion_di: np.ndarray            # [nions] dere_di_flag
+    ion_dr: np.ndarray            # [nions] drflag
+    inner_nion: np.ndarray        # [n_inner] ion an inner-shell rate depopulates
+    inner_yield: np.ndarray       # [n_inner] row of yield_prob, -1 without yield data
+    yield_prob: np.ndarray        # [n_yield, 10] probability of 1..10 ejected electrons
+    cx_nion1: np.ndarray          # [ncx] ion ionised by charge exchange
+    cx_nion2: np.ndarray          # [ncx] its partner (hydrogen for the rates that count)
+
+    @property
+    def nions(self) -> int:
+        return int(self.ion_istate.size)
+
+    @property
+    def nelem(self) -> int:
+        return int(self.elem_z.size)
+
+    @property
+    def n_inner(self) -> int:
+        return int(self.inner_nion.size)
+
+    @property
+    def ncx(self) -> int:
+        return int(self.cx_nion1.size)
+
+    def elem_of(self) -> np.ndarray:
+        e = np.empty(self.nions, dtype=np.int32)
+        for k in range(self.nelem):
+            e[self.elem_first[k]:self.elem_first[k] + self.elem_n[k]] = k
+        return e
+
+
+@dataclass
+class IonRates:
+    """Per-cell coefficients of populate_ion_rate_matrix: photoionisation (pi),
+    radiative recombination (rr), direct-ionisation, three-body and dielectronic
+    coefficients (di, qr, dr; the reference's di_coeffs / qrecomb_coeffs /
+    dr_coeffs), charge-exchange recombination per ion (cxr) and ionisation per
+    charge-exchange entry (cxi), inner-shell rates (inner)."""
+    pi: np.ndarray
+    rr: np.ndarray
+    di: np.ndarray
+    qr: np.ndarray
+    dr: np.ndarray
+    cxr: np.ndarray
+    cxi: np.ndarray
+    inner: np.ndarray
+
+    @property
+    def ncell(self) -> int:
+        return int(self.pi.shape[0])
+
+
+def ion_table(zs=(1, 2, 6, 8, 26), seed: int = BASE_SEED + 5) -> IonTable:
+    """Synthetic atomic table: every stage of each element from neutral to bare
+    (Z + 1 ions), random DI / DR flags, 0-3 inner-shell rates for ions with at
+    least three electrons (a fifth without yield data), and charge-exchange
+    ionisation of metal ions against H II plus entries with other partners
+    (which the reference skips)."""
+    rng = np.random.default_rng(seed)
+    elem_z = np.array(zs, dtype=np.int32)
+    elem_n = elem_z + 1
+    elem_first = np.concatenate([[0], np.cumsum(elem_n)[:-1]]).astype(np.int32)
+    nions = int(elem_n.sum())
+    ion_istate = np.concatenate([np.arange(1, z + 2) for z in zs]).astype(np.int32)
+    ion_di = (rng.random(nions) < 0.5).astype(np.int32)
+    ion_dr = (rng.random(nions) < 0.6).astype(np.int32) * rng.integers(1, 3, nions).astype(np.int32)
+    z_of = np.repeat(elem_z, elem_n)
+    inner_nion, inner_yield, probs = [], [], []
+    for i in range(nions):
+        if z_of[i] - ion_istate[i] + 1 >= 3:
+            for _ in range(int(rng.integers(0, 4))):
+                inner_nion.append(i)
+                if rng.random() < 0.2:
+                    inner_yield.append(-1)
+                else:
+                    p = rng.random(10)
+                    probs.append(p / p.sum() * rng.uniform(0.5, 1.0))
+                    inner_yield.append(len(probs) - 1)
+    h_ii = int(elem_first[list(zs).index(1)] + 1) if 1 in zs else 0
+    cx1, cx2 = [], []
+    for e, z in enumerate(zs):
+        if z == 1:
+            continue
+        for i in range(int(elem_first[e]), int(elem_first[e] + elem_n[e]) - 1):
+            if rng.random() < 0.3:
+                cx1.append(i)
+                cx2.append(h_ii if rng.random() < 0.8 else int(elem_first[e]))
+    return IonTable(elem_z, elem_first, elem_n.astype(np.int32), (elem_z + 1).astype(np.int32), ion_istate, ion_di,
+                    ion_dr, np.array(inner_nion, dtype=np.int32), np.array(inner_yield, dtype=np.int32),
+                    np.array(probs, dtype=np.float64).reshape(-1, 10), np.array(cx1, dtype=np.int32),
+                    np.array(cx2, dtype=np.int32))
+
+
+def ion_rates(tab: IonTable, ncell: int, seed: int = BASE_SEED + 6) -> IonRates:
+    """Log-uniform coefficients per cell; charge-exchange recombination is zero
+    for hydrogen and neutral ions (nothing to recombine into)."""
+    rng = np.random.default_rng(seed)
+    n = tab.nions
+
+    def lu(lo, hi, shape):
+        return np.exp(rng.uniform(np.log(lo), np.log(hi), shape))
+    cxr = lu(1e-12, 1e-8, (ncell, n))
+    z_of = np.repeat(tab.elem_z, tab.elem_n)
+    cxr[:, (z_of == 1) | (tab.ion_istate == 1)] = 0.0
+    return IonRates(pi=lu(1e-8, 1e2, (ncell, n)), rr=lu(1e-14, 1e-10, (ncell, n)), di=lu(1e-16, 1e-8, (ncell, n)),
+                    qr=lu(1e-30, 1e-24, (ncell, n)), dr=lu(1e-14, 1e-10, (ncell, n)), cxr=cxr,
+                    cxi=lu(1e-12, 1e-8, (ncell, tab.ncx)), inner=lu(1e-6, 1e-1, (ncell, tab.n_inner)))
