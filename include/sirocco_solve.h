@@ -182,6 +182,50 @@ typedef struct sirocco_ion_rates {
 int ion_rate_matrices_batched(const sirocco_ion_table *tab, int ncell, const sirocco_ion_rates *rates,
                               const double *ne, const double *nh1, const double *nh2, double *A, double *b);
 
+/* A macro-atom model as calc_matom_matrix (source/macro_accelerate.c:31-348)
+   walks it.  Level u's jumps, each list in the reference's order, are entries
+   [x_start[u], x_start[u+1]) of the matching target arrays: downward
+   bound-bound (bbd: the line's lower level), Auger (aug: target level and
+   Avalue_auger * branching_ratio), downward bound-free (bfd: the continuum's
+   lower level), upward bound-bound (bbu: the line's upper level), upward
+   bound-free (bfu: the continuum's upper level).  The k-packet row takes the
+   macro lines' (kbb) and macro continua's (kbf) upper levels, in line and
+   continuum order.  Host arrays. */
+typedef struct sirocco_matom_table {
+  int nlev;                                   /* nlevels_macro; the k-packet is row and column nlev */
+  const double *ex;                           /* [nlev] level energies */
+  const int *bbd_start, *bbd_target;          /* [nlev + 1], [bbd_start[nlev]] */
+  const int *aug_start, *aug_target;
+  const double *aug_rate;
+  const int *bfd_start, *bfd_target;
+  const int *bbu_start, *bbu_target;
+  const int *bfu_start, *bfu_target;
+  int n_kbb, n_kbf;
+  const int *kbb_target, *kbf_target;
+} sirocco_matom_table;
+
+/* Per-cell coefficients, cell after cell, one per jump of the matching list:
+   bbd_rad = a21 * p_escape and bbd_coll = q21; bfd_sp = recomb_sp and bfd_qrec
+   = q_recomb; bbu_rad = b12 * jbar and bbu_coll = q12; bfu_gamma, bfu_alpha
+   (alpha_st), bfu_ratio (upper / lower level density, zero below
+   DENSITY_PHOT_MIN) and bfu_qion = q_ioniz; kbb / kbf the cooling rates of the
+   macro lines / continua (cooling_bb, cooling_bf_col); kr the k-packet to
+   r-packet rate summed as the reference sums it; ne the electron density (one
+   per cell). */
+typedef struct sirocco_matom_rates {
+  const double *bbd_rad, *bbd_coll, *bfd_sp, *bfd_qrec, *bbu_rad, *bbu_coll;
+  const double *bfu_gamma, *bfu_alpha, *bfu_ratio, *bfu_qion, *kbb, *kbf, *kr, *ne;
+} sirocco_matom_rates;
+
+/* The Q / R assembly and normalisation of calc_matom_matrix
+   (macro_accelerate.c:82-284) on the GPU for ncell cells: N = I - Q / Q_norm,
+   (nlev + 1)^2 row-major per cell, and the diagonal of R / Q_norm, nlev + 1
+   per cell, each bit-identical to the reference's.  N and R may be host or
+   device pointers; device outputs feed matom_matrices_batched directly.
+   Targets outside 0..nlev-1 return SIROCCO_EINVAL. */
+int matom_rate_matrices_batched(const sirocco_matom_table *tab, int ncell, const sirocco_matom_rates *rates,
+                                double *N, double *R);
+
 /* ion_populations_lockstep with the rate matrices assembled on the GPU from
    `tab` and `rates` each round (only n_e and the hydrogen densities change
    between rounds), so no matrix crosses the bus.  Same outputs and rules. */

@@ -234,3 +234,161 @@ def ref_ion_rate_matrix(tab, rates, cell: int, xne: float, nh1: float, nh2: floa
            ctypes.c_double(xne), ctypes.c_double(nh1), ctypes.c_double(nh2), _p(A), _p(b))
     del keep
     return A, b, rc
+
+
+# ------------------------------------------------- macro-atom jump matrices --
+MATOM_LIB = HERE / "_ref" / "libref_matom.so"
+
+
+def matom_density_ratio(m, cell, density_phot_min: float = 1e-10):
+    """Per upward bound-free jump, the upper / lower density ratio of
+    calc_matom_matrix (macro_accelerate.c:203-210): zero below DENSITY_PHOT_MIN."""
+    out = []
+    for u in range(m.nlev):
+        for i in m.bfu[u]:
+            lo = float(cell.den[m.phot_lo[i]])
+            out.append(float(cell.den[m.phot_up[i]]) / lo if lo >= density_phot_min else 0.0)
+    return np.array(out, dtype=np.float64)
+
+
+def matom_kr(m, cell) -> float:
+    """The k-packet to r-packet rate of calc_matom_matrix (:224-254), summed in
+    the routine's order: simple lines, simple continua, then the other coolings."""
+    kr = 0.0
+    for i in range(m.line_lo.size):
+        if not m.line_macro[i]:
+            kr += float(cell.cool_bb[i])
+    for i in range(m.phot_lo.size):
+        if not m.phot_macro[i]:
+            kr += float(cell.cool_bf[i])
+    kr += cell.cool_bftot
+    kr += cell.cool_adiabatic
+    kr += cell.cool_ff + cell.cool_ff_lofreq
+    return kr
+
+
+def matom_rate_matrix(m, cell, density_phot_min: float = 1e-10):
+    """Restatement of the Q / R assembly and normalisation of calc_matom_matrix
+    (source/macro_accelerate.c:82-300) for one cell: N = I - Q / Q_norm
+    ((nlev + 1)^2, row-major, the k-packet row and column last) and the
+    diagonal of R / Q_norm.  Each sum and product is rounded separately, in the
+    routine's order."""
+    n = m.nlev
+    K = n
+    ex = [float(v) for v in m.ex]
+    ne = float(cell.ne)
+    Q = [[0.0] * (n + 1) for _ in range(n + 1)]
+    R = [0.0] * (n + 1)
+    qn = [0.0] * (n + 1)
+    ratio = matom_density_ratio(m, cell, density_phot_min)
+    ibu = ifu = ifd = 0
+    for u in range(n):
+        for i in m.bbd[u]:                                   # bound-bound down (:98-123)
+            rad = float(cell.a21[i]) * float(cell.pesc[i])
+            coll = float(cell.q21[i])
+            bb = rad + coll * ne
+            t = int(m.line_lo[i])
+            qc = bb * ex[t]
+            Q[u][t] += qc
+            qk = (coll * ne) * (ex[u] - ex[t])
+            Q[u][K] += qk
+            rc = rad * (ex[u] - ex[t])
+            R[u] += rc
+            qn[u] += qc + qk + rc
+        if m.aug_idx[u] >= 0:                                # Auger (:126-145)
+            a = int(m.aug_idx[u])
+            for k in range(int(m.n_aug[u])):
+                t = int(m.aug_target[a][k])
+                rate = float(m.aug_A[a]) * float(m.aug_branch[a][k])
+                qc = rate * ex[t]
+                Q[u][t] += qc
+                qk = rate * (ex[u] - ex[t])
+                Q[u][K] += qk
+                qn[u] += qc + qk
+        for i in m.bfd[u]:                                   # bound-free down (:148-174)
+            sp = float(cell.recomb_sp[ifd])
+            ifd += 1
+            qr = float(cell.qrec[i])
+            bf = (sp + qr * ne) * ne
+            t = int(m.phot_lo[i])
+            if bf > 0.0:
+                qc = bf * ex[t]
+                Q[u][t] += qc
+                qk = qr * ne * ne * (ex[u] - ex[t])
+                Q[u][K] += qk
+                rc = ne * sp * (ex[u] - ex[t])
+                R[u] += rc
+                qn[u] += qc + qk + rc
+        for i in m.bbu[u]:                                   # bound-bound up (:179-191)
+            rad = float(cell.b12[i]) * float(cell.jbar[ibu])
+            ibu += 1
+            coll = float(cell.q12[i])
+            t = int(m.line_up[i])
+            qc = (rad + coll * ne) * ex[u]
+            Q[u][t] += qc
+            qn[u] += qc
+        for i in m.bfu[u]:                                   # bound-free up (:194-222)
+            t = int(m.phot_up[i])
+            qc = (float(cell.gamma[ifu]) - float(cell.alpha_st[ifu]) * ne * float(ratio[ifu]) +
+                  float(cell.qion[i]) * ne) * ex[u]
+            ifu += 1
+            if qc < 0.0:
+                qc = 0.0
+            Q[u][t] += qc
+            qn[u] += qc
+    for i in range(m.line_lo.size):                          # k-packet row (:236-263)
+        if m.line_macro[i]:
+            qc = float(cell.cool_bb[i])
+            Q[K][int(m.line_up[i])] += qc
+            qn[K] += qc
+    for i in range(m.phot_lo.size):
+        if m.phot_macro[i]:
+            qc = float(cell.cool_bf[i])
+            Q[K][int(m.phot_up[i])] += qc
+            qn[K] += qc
+    kr = matom_kr(m, cell)
+    R[K] += kr
+    qn[K] += kr
+    for u in range(n + 1):                                   # N = I - Q / Q_norm (:270-284)
+        for t in range(n + 1):
+            if qn[u] > 0.0:
+                Q[u][t] = -1.0 * Q[u][t] / qn[u]
+        Q[u][u] = 1.0
+        if qn[u] > 0.0:
+            R[u] = R[u] / qn[u]
+    return np.array(Q, dtype=np.float64), np.array(R, dtype=np.float64)
+
+
+def matom_reference_available() -> bool:
+    return MATOM_LIB.exists()
+
+
+def ref_matom_b(m, cell, density_phot_min: float = 1e-10):
+    """The reference's own calc_matom_matrix (oracle/_ref/libref_matom.so) on the
+    same model and coefficients: B = N^-1 diag(R), (nlev + 1)^2 row-major."""
+    lib = ctypes.CDLL(str(MATOM_LIB))
+    f = lib.refmatom_b
+    f.restype = c_int
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    n = m.nlev
+    cnt = lambda L: i32([len(v) for v in L])
+    flat = lambda L: i32([i for v in L for i in v] or [0])
+    arrs = [f64(m.ex), cnt(m.bbd), flat(m.bbd), cnt(m.bbu), flat(m.bbu), cnt(m.bfd), flat(m.bfd), cnt(m.bfu),
+            flat(m.bfu), i32(m.aug_idx), i32(m.n_aug)]
+    aug = [i32(m.aug_target.reshape(-1) if m.aug_target.size else [0]), f64(m.aug_A if m.aug_A.size else [0.0]),
+           f64(m.aug_branch.reshape(-1) if m.aug_branch.size else [0.0])]
+    lines = [i32(m.line_lo), i32(m.line_up), i32(m.line_macro)]
+    phots = [i32(m.phot_lo), i32(m.phot_up), i32(m.phot_macro)]
+    coef = [f64(getattr(cell, k)) for k in ("a21", "pesc", "q21", "b12", "q12", "qrec", "qion", "jbar", "gamma",
+                                             "alpha_st", "recomb_sp", "den", "cool_bb", "cool_bf")]
+    coef = [c if c.size else f64([0.0]) for c in coef]
+    B = np.zeros((n + 1) * (n + 1), dtype=np.float64)
+    rc = f(c_int(n), *[_p(a) for a in arrs], c_int(int(m.aug_A.size)), *[_p(a) for a in aug],
+           c_int(int(m.line_lo.size)), *[_p(a) for a in lines], c_int(int(m.phot_lo.size)), *[_p(a) for a in phots],
+           *[_p(a) for a in coef], ctypes.c_double(cell.cool_bftot), ctypes.c_double(cell.cool_adiabatic),
+           ctypes.c_double(cell.cool_ff), ctypes.c_double(cell.cool_ff_lofreq), ctypes.c_double(cell.t_e),
+           ctypes.c_double(cell.ne), ctypes.c_double(density_phot_min), _p(B))
+    if rc != 0:
+        raise RuntimeError(f"refmatom_b returned {rc}")
+    return B.reshape(n + 1, n + 1)

@@ -28,6 +28,7 @@
 #include "kernels_global.cuh"
 #include "kernels_ionasm.cuh"
 #include "kernels_matom.cuh"
+#include "kernels_matomasm.cuh"
 #include "kernels_mixed.cuh"
 #include "kernels_small.cuh"
 
@@ -454,6 +455,7 @@ struct Context {
   DevBuf bA, bb, bx, bst;
   DevBuf bR, bC, bOv, bN, bOa, bQs, bQl, bQz, bQt;   // macro-atom epilogue and draws
   DevBuf bIT, bI64, bID, bIL, bIS, bIA, bIB, bIX, bISt;   // ion rate-matrix assembly
+  DevBuf bMT, bMD, bMN, bMR;                              // macro-atom jump-matrix assembly
   int mode = SIROCCO_FP64;
   ~Context() { release(); }
   void release() {
@@ -1188,6 +1190,154 @@ static int run_ion_lockstep_rates(const sirocco_ion_table* t, int ncell, const s
                            ne, den, round, status, iters);
 }
 
+// ------------------------------------------- macro-atom jump-matrix assembly --
+static int run_matom_rate_matrices(const sirocco_matom_table* t, int ncell, const sirocco_matom_rates* r, double* N,
+                                   double* R) {
+  if (ncell == 0) return 0;
+  if (ncell < 0 || !t || !r || !N || !R || t->nlev < 1 || !t->ex || !t->bbd_start || !t->aug_start ||
+      !t->bfd_start || !t->bbu_start || !t->bfu_start || t->n_kbb < 0 || t->n_kbf < 0 ||
+      (t->n_kbb > 0 && !t->kbb_target) || (t->n_kbf > 0 && !t->kbf_target) || !r->kr || !r->ne) {
+    set_error("invalid macro-atom table or rates");
+    return SIROCCO_EINVAL;
+  }
+  const int nlev = t->nlev;
+  // each jump list: its starts ascend from 0 and its targets are levels
+  const int* starts[5] = {t->bbd_start, t->aug_start, t->bfd_start, t->bbu_start, t->bfu_start};
+  const int* targets[5] = {t->bbd_target, t->aug_target, t->bfd_target, t->bbu_target, t->bfu_target};
+  int cnt[5];
+  for (int l = 0; l < 5; ++l) {
+    if (starts[l][0] != 0) {
+      set_error("jump list %d does not start at 0", l);
+      return SIROCCO_EINVAL;
+    }
+    for (int u = 0; u < nlev; ++u)
+      if (starts[l][u + 1] < starts[l][u]) {
+        set_error("jump list %d: starts descend at level %d", l, u);
+        return SIROCCO_EINVAL;
+      }
+    cnt[l] = starts[l][nlev];
+    if (cnt[l] > 0 && !targets[l]) {
+      set_error("jump list %d has no targets", l);
+      return SIROCCO_EINVAL;
+    }
+    for (int j = 0; j < cnt[l]; ++j)
+      if (targets[l][j] < 0 || targets[l][j] >= nlev) {
+        set_error("jump list %d: target %d of jump %d outside 0..%d", l, targets[l][j], j, nlev - 1);
+        return SIROCCO_EINVAL;
+      }
+  }
+  for (int j = 0; j < t->n_kbb; ++j)
+    if (t->kbb_target[j] < 0 || t->kbb_target[j] >= nlev) {
+      set_error("k-packet line %d: target %d outside 0..%d", j, t->kbb_target[j], nlev - 1);
+      return SIROCCO_EINVAL;
+    }
+  for (int j = 0; j < t->n_kbf; ++j)
+    if (t->kbf_target[j] < 0 || t->kbf_target[j] >= nlev) {
+      set_error("k-packet continuum %d: target %d outside 0..%d", j, t->kbf_target[j], nlev - 1);
+      return SIROCCO_EINVAL;
+    }
+  const int n_bbd = cnt[0], n_aug = cnt[1], n_bfd = cnt[2], n_bbu = cnt[3], n_bfu = cnt[4];
+  if ((n_aug > 0 && !t->aug_rate) || (n_bbd > 0 && (!r->bbd_rad || !r->bbd_coll)) ||
+      (n_bfd > 0 && (!r->bfd_sp || !r->bfd_qrec)) || (n_bbu > 0 && (!r->bbu_rad || !r->bbu_coll)) ||
+      (n_bfu > 0 && (!r->bfu_gamma || !r->bfu_alpha || !r->bfu_ratio || !r->bfu_qion)) ||
+      (t->n_kbb > 0 && !r->kbb) || (t->n_kbf > 0 && !r->kbf)) {
+    set_error("missing macro-atom coefficients");
+    return SIROCCO_EINVAL;
+  }
+  Context* c = ctx();
+  int rc = c->init();
+  if (rc) return rc;
+  // ints: five (starts, targets) pairs, then the k-packet targets
+  std::vector<int> ints;
+  std::vector<size_t> io;
+  auto put_i = [&](const int* p, size_t k) {
+    io.push_back(ints.size());
+    if (k) ints.insert(ints.end(), p, p + k);
+  };
+  for (int l = 0; l < 5; ++l) {
+    put_i(starts[l], size_t(nlev) + 1);
+    put_i(targets[l], size_t(cnt[l]));
+  }
+  put_i(t->kbb_target, size_t(t->n_kbb));
+  put_i(t->kbf_target, size_t(t->n_kbf));
+  // doubles: ex, aug_rate, then the per-cell coefficients
+  const size_t nc = size_t(ncell);
+  const size_t dsz[] = {size_t(nlev), size_t(n_aug), nc * n_bbd, nc * n_bbd, nc * n_bfd, nc * n_bfd, nc * n_bbu,
+                        nc * n_bbu, nc * n_bfu, nc * n_bfu, nc * n_bfu, nc * n_bfu, nc * t->n_kbb, nc * t->n_kbf,
+                        nc, nc};
+  const double* dsrc[] = {t->ex, t->aug_rate, r->bbd_rad, r->bbd_coll, r->bfd_sp, r->bfd_qrec, r->bbu_rad,
+                          r->bbu_coll, r->bfu_gamma, r->bfu_alpha, r->bfu_ratio, r->bfu_qion, r->kbb, r->kbf, r->kr,
+                          r->ne};
+  constexpr int ND = int(sizeof(dsz) / sizeof(dsz[0]));
+  size_t dtot = 0;
+  for (size_t k : dsz) dtot += k;
+  const int nr = nlev + 1;
+  const bool devN = is_device_ptr(N), devR = is_device_ptr(R);
+  if ((rc = c->bMT.ensure(sizeof(int) * std::max<size_t>(ints.size(), 1))) ||
+      (rc = c->bMD.ensure(sizeof(double) * std::max<size_t>(dtot, 1))) ||
+      (!devN && (rc = c->bMN.ensure(sizeof(double) * nc * nr * nr))) ||
+      (!devR && (rc = c->bMR.ensure(sizeof(double) * nc * nr))))
+    return rc;
+  int* di_ = static_cast<int*>(c->bMT.ptr);
+  double* dd = static_cast<double*>(c->bMD.ptr);
+  SS_CUDA(cudaMemcpy(di_, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice));
+  const double* dp[ND];
+  size_t off = 0;
+  for (int k = 0; k < ND; ++k) {
+    dp[k] = dd + off;
+    if (dsz[k] > 0) SS_CUDA(cudaMemcpy(dd + off, dsrc[k], sizeof(double) * dsz[k], cudaMemcpyHostToDevice));
+    off += dsz[k];
+  }
+  MatomAsmView v{};
+  v.nlev = nlev;
+  v.n_bbd = n_bbd;
+  v.n_aug = n_aug;
+  v.n_bfd = n_bfd;
+  v.n_bbu = n_bbu;
+  v.n_bfu = n_bfu;
+  v.n_kbb = t->n_kbb;
+  v.n_kbf = t->n_kbf;
+  v.bbd_start = di_ + io[0];
+  v.bbd_t = di_ + io[1];
+  v.aug_start = di_ + io[2];
+  v.aug_t = di_ + io[3];
+  v.bfd_start = di_ + io[4];
+  v.bfd_t = di_ + io[5];
+  v.bbu_start = di_ + io[6];
+  v.bbu_t = di_ + io[7];
+  v.bfu_start = di_ + io[8];
+  v.bfu_t = di_ + io[9];
+  v.kbb_t = di_ + io[10];
+  v.kbf_t = di_ + io[11];
+  v.ex = dp[0];
+  v.aug_rate = dp[1];
+  v.bbd_rad = dp[2];
+  v.bbd_coll = dp[3];
+  v.bfd_sp = dp[4];
+  v.bfd_qrec = dp[5];
+  v.bbu_rad = dp[6];
+  v.bbu_coll = dp[7];
+  v.bfu_gamma = dp[8];
+  v.bfu_alpha = dp[9];
+  v.bfu_ratio = dp[10];
+  v.bfu_qion = dp[11];
+  v.kbb = dp[12];
+  v.kbf = dp[13];
+  v.kr = dp[14];
+  v.ne = dp[15];
+  v.ncell = ncell;
+  v.N = devN ? N : static_cast<double*>(c->bMN.ptr);
+  v.R = devR ? R : static_cast<double*>(c->bMR.ptr);
+  const int64_t threads = int64_t(ncell) * nr;
+  matom_assemble_kernel<<<unsigned((threads + kMatomAsmThreads - 1) / kMatomAsmThreads), kMatomAsmThreads, 0,
+                          c->stream>>>(v);
+  SS_CUDA(cudaGetLastError());
+  if (!devN) SS_CUDA(cudaMemcpyAsync(N, v.N, sizeof(double) * nc * nr * nr, cudaMemcpyDeviceToHost, c->stream));
+  if (!devR) SS_CUDA(cudaMemcpyAsync(R, v.R, sizeof(double) * nc * nr, cudaMemcpyDeviceToHost, c->stream));
+  SS_CUDA(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
 // --------------------------------------------------------- macro-atom pops --
 // macro_pops (source/macro_gov.c:336-505) for one macro element over many cells:
 // each round solves the level systems of every unfinished cell in one batched
@@ -1488,6 +1638,11 @@ int ion_populations_lockstep(int ncell, int nions, int nelem, const int* elem_fi
                              sirocco_ion_assemble_fn assemble, void* user, int* status, int* iters) {
   return ss::run_ion_lockstep(ncell, nions, nelem, elem_first, elem_n, istate, h_elem, elem_dens, ne, den, assemble,
                               user, status, iters);
+}
+
+int matom_rate_matrices_batched(const sirocco_matom_table* tab, int ncell, const sirocco_matom_rates* rates, double* N,
+                                double* R) {
+  return ss::run_matom_rate_matrices(tab, ncell, rates, N, R);
 }
 
 int ion_rate_matrices_batched(const sirocco_ion_table* tab, int ncell, const sirocco_ion_rates* rates, const double* ne,

@@ -30,7 +30,7 @@ EXPORTS = (
     "sirocco_plan_create", "sirocco_plan_execute", "sirocco_plan_launches",
     "sirocco_plan_destroy", "sirocco_last_error", "solve_matrix_batched_noalloc",
     "matom_matrices_batched", "matom_sample_batched", "ion_populations_lockstep", "macro_pops_lockstep",
-    "ion_rate_matrices_batched", "ion_populations_lockstep_rates",
+    "ion_rate_matrices_batched", "ion_populations_lockstep_rates", "matom_rate_matrices_batched",
 )
 
 _lib = None
@@ -53,6 +53,24 @@ class IonTableC(ctypes.Structure):
 class IonRatesC(ctypes.Structure):
     """sirocco_ion_rates (include/sirocco_solve.h)."""
     _fields_ = [(k, c_void_p) for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")]
+
+
+class MatomTableC(ctypes.Structure):
+    """sirocco_matom_table (include/sirocco_solve.h)."""
+    _fields_ = [("nlev", c_int), ("ex", c_void_p), ("bbd_start", c_void_p), ("bbd_target", c_void_p),
+                ("aug_start", c_void_p), ("aug_target", c_void_p), ("aug_rate", c_void_p), ("bfd_start", c_void_p),
+                ("bfd_target", c_void_p), ("bbu_start", c_void_p), ("bbu_target", c_void_p), ("bfu_start", c_void_p),
+                ("bfu_target", c_void_p), ("n_kbb", c_int), ("n_kbf", c_int), ("kbb_target", c_void_p),
+                ("kbf_target", c_void_p)]
+
+
+MATOM_RATE_FIELDS = ("bbd_rad", "bbd_coll", "bfd_sp", "bfd_qrec", "bbu_rad", "bbu_coll", "bfu_gamma", "bfu_alpha",
+                     "bfu_ratio", "bfu_qion", "kbb", "kbf", "kr", "ne")
+
+
+class MatomRatesC(ctypes.Structure):
+    """sirocco_matom_rates (include/sirocco_solve.h)."""
+    _fields_ = [(k, c_void_p) for k in MATOM_RATE_FIELDS]
 
 
 class EngineError(RuntimeError):
@@ -110,6 +128,8 @@ def load() -> ctypes.CDLL:
     lib.ion_populations_lockstep_rates.argtypes = [POINTER(IonTableC), c_int, POINTER(IonRatesC), c_int] + \
         [c_void_p] * 5
     lib.ion_populations_lockstep_rates.restype = c_int
+    lib.matom_rate_matrices_batched.argtypes = [POINTER(MatomTableC), c_int, POINTER(MatomRatesC), c_void_p, c_void_p]
+    lib.matom_rate_matrices_batched.restype = c_int
     lib.macro_pops_lockstep.argtypes = [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                         MACRO_ASSEMBLE_FN, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.macro_pops_lockstep.restype = c_int
@@ -280,6 +300,32 @@ def _ion_c(tab, rates):
     rk = {k: f64(getattr(rates, k)) for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")}
     r = IonRatesC(*[rk[k].ctypes.data for k in ("pi", "rr", "di", "qr", "dr", "cxr", "cxi", "inner")])
     return t, r, (keep, rk)
+
+
+def matom_rate_matrices(inp: dict, N=None, R=None):
+    """The Q / R assembly and normalisation of calc_matom_matrix on the GPU
+    (matom_rate_matrices_batched) from workloads.matom_jump_inputs arrays:
+    returns (N [ncell, nlev+1, nlev+1], R [ncell, nlev+1]).  N and R may be
+    given as device tensors (torch) to keep the result on the GPU."""
+    lib = load()
+    nlev, ncell = int(inp["nlev"]), int(inp["ncell"])
+    a = {k: np.ascontiguousarray(v) for k, v in inp.items() if isinstance(v, np.ndarray)}
+    ptr = lambda k: a[k].ctypes.data if a[k].size else None
+    t = MatomTableC(nlev, ptr("ex"), ptr("bbd_start"), ptr("bbd_target"), ptr("aug_start"), ptr("aug_target"),
+                    ptr("aug_rate"), ptr("bfd_start"), ptr("bfd_target"), ptr("bbu_start"), ptr("bbu_target"),
+                    ptr("bfu_start"), ptr("bfu_target"), int(a["kbb_target"].size), int(a["kbf_target"].size),
+                    ptr("kbb_target"), ptr("kbf_target"))
+    r = MatomRatesC(*[ptr(k) for k in MATOM_RATE_FIELDS])
+    nr = nlev + 1
+    if N is None:
+        N = np.empty((ncell, nr, nr), np.float64)
+        R = np.empty((ncell, nr), np.float64)
+        pn, pr = _ptr(N), _ptr(R)
+    else:
+        pn, pr = c_void_p(N.data_ptr()), c_void_p(R.data_ptr())
+    rc = lib.matom_rate_matrices_batched(ctypes.byref(t), ncell, ctypes.byref(r), pn, pr)
+    _check(rc, "matom_rate_matrices_batched")
+    return N, R
 
 
 def ion_rate_matrices(tab, rates, ne, nh1, nh2):

@@ -382,3 +382,212 @@ def ion_rates(tab: IonTable, ncell: int, seed: int = BASE_SEED + 6) -> IonRates:
     return IonRates(pi=lu(1e-8, 1e2, (ncell, n)), rr=lu(1e-14, 1e-10, (ncell, n)), di=lu(1e-16, 1e-8, (ncell, n)),
                     qr=lu(1e-30, 1e-24, (ncell, n)), dr=lu(1e-14, 1e-10, (ncell, n)), cxr=cxr,
                     cxi=lu(1e-12, 1e-8, (ncell, tab.ncx)), inner=lu(1e-6, 1e-1, (ncell, tab.n_inner)))
+
+
+# ------------------------------------------- macro-atom jump tables and rates --
+@dataclass
+class MatomModel:
+    """A macro-atom model as calc_matom_matrix (source/macro_accelerate.c:31-348)
+    walks it: levels with energies, lines and continua between levels (macro
+    or simple), per-level jump lists in the reference's order, Auger entries."""
+    ex: np.ndarray           # [nlev] level energies
+    line_lo: np.ndarray      # [nline]
+    line_up: np.ndarray
+    line_macro: np.ndarray
+    phot_lo: np.ndarray      # [nphot]
+    phot_up: np.ndarray
+    phot_macro: np.ndarray
+    bbd: list                # per level: line indices of its downward bound-bound jumps
+    bbu: list                # per level: line indices of its upward ones
+    bfd: list                # per level: continuum indices of its downward bound-free jumps
+    bfu: list                # per level: upward ones
+    aug_idx: np.ndarray      # [nlev] Auger entry of the level, -1 without
+    n_aug: np.ndarray        # [nlev] Auger channels used
+    aug_target: np.ndarray   # [naug, 4]
+    aug_A: np.ndarray        # [naug]
+    aug_branch: np.ndarray   # [naug, 4]
+
+    @property
+    def nlev(self) -> int:
+        return int(self.ex.size)
+
+
+@dataclass
+class MatomCell:
+    """One cell's coefficients: a21, p_escape, q21, b12, q12 per line; q_recomb,
+    q_ioniz per continuum; jbar per upward bound-bound jump, gamma and alpha_st
+    per upward bound-free jump, recomb_sp per downward bound-free jump (levels
+    in order); den per level; the k-packet cooling rates; t_e and n_e."""
+    a21: np.ndarray
+    pesc: np.ndarray
+    q21: np.ndarray
+    b12: np.ndarray
+    q12: np.ndarray
+    qrec: np.ndarray
+    qion: np.ndarray
+    jbar: np.ndarray
+    gamma: np.ndarray
+    alpha_st: np.ndarray
+    recomb_sp: np.ndarray
+    den: np.ndarray
+    cool_bb: np.ndarray
+    cool_bf: np.ndarray
+    cool_bftot: float
+    cool_adiabatic: float
+    cool_ff: float
+    cool_ff_lofreq: float
+    t_e: float
+    ne: float
+
+
+def matom_model(ion_levels=(12, 20, 16, 9, 1), seed: int = BASE_SEED + 7) -> MatomModel:
+    """Synthetic macro atom: ions of the given level counts, energies rising
+    within and across ions; lines between levels of one ion (one in six
+    simple), continua from each level of an ion to levels of the next (all
+    macro but the highest ion's), a few Auger-capable levels."""
+    rng = np.random.default_rng(seed)
+    first = np.concatenate([[0], np.cumsum(ion_levels)[:-1]]).astype(int)
+    ex = []
+    base = 0.0
+    for k, nl in enumerate(ion_levels):
+        ex += list(base + np.sort(rng.uniform(0.0, 1e-11, nl)) * (1 if nl > 1 else 0))
+        base += 2e-11
+    ex = np.array(ex)
+    nlev = ex.size
+    lo, up, mac = [], [], []
+    for k, nl in enumerate(ion_levels):
+        for a in range(nl):
+            for b in range(a + 1, nl):
+                if rng.random() < 0.35:
+                    lo.append(first[k] + a)
+                    up.append(first[k] + b)
+                    mac.append(0 if rng.random() < 1 / 6 else 1)
+    plo, pup, pmac = [], [], []
+    for k in range(len(ion_levels) - 1):
+        for a in range(ion_levels[k]):
+            for b in range(min(2, ion_levels[k + 1])):
+                if b == 0 or rng.random() < 0.3:
+                    plo.append(first[k] + a)
+                    pup.append(first[k + 1] + b)
+                    pmac.append(1)
+    line_lo, line_up, line_macro = (np.array(v, dtype=np.int32) for v in (lo, up, mac))
+    phot_lo, phot_up, phot_macro = (np.array(v, dtype=np.int32) for v in (plo, pup, pmac))
+    bbd = [[i for i in range(line_lo.size) if line_up[i] == u and line_macro[i]] for u in range(nlev)]
+    bbu = [[i for i in range(line_lo.size) if line_lo[i] == u and line_macro[i]] for u in range(nlev)]
+    bfd = [[i for i in range(phot_lo.size) if phot_up[i] == u and phot_macro[i]] for u in range(nlev)]
+    bfu = [[i for i in range(phot_lo.size) if phot_lo[i] == u and phot_macro[i]] for u in range(nlev)]
+    aug_idx = np.full(nlev, -1, dtype=np.int32)
+    n_aug = np.zeros(nlev, dtype=np.int32)
+    tg, A, br = [], [], []
+    for u in rng.choice(nlev - ion_levels[-1], size=3, replace=False):
+        k = int(np.searchsorted(first, u, side="right") - 1)
+        if k + 2 >= len(ion_levels):
+            continue
+        aug_idx[u] = len(A)
+        n_aug[u] = int(rng.integers(1, 5))
+        tg.append([first[k + 2] + int(rng.integers(0, ion_levels[k + 2])) for _ in range(4)])
+        A.append(float(10 ** rng.uniform(10, 14)))
+        p = rng.random(4)
+        br.append(p / p.sum())
+    return MatomModel(ex, line_lo, line_up, line_macro, phot_lo, phot_up, phot_macro, bbd, bbu, bfd, bfu, aug_idx,
+                      n_aug, np.array(tg, dtype=np.int32).reshape(-1, 4), np.array(A, dtype=np.float64),
+                      np.array(br, dtype=np.float64).reshape(-1, 4))
+
+
+def matom_cell(m: MatomModel, seed: int) -> MatomCell:
+    """Log-uniform coefficients for one cell; a few upward bound-free jumps get
+    a stimulated-recombination term large enough to make their rate negative
+    (the reference clamps it to zero), a few downward ones a zero rate."""
+    rng = np.random.default_rng(seed)
+    nl, npht = m.line_lo.size, m.phot_lo.size
+    nbu = sum(len(v) for v in m.bbu)
+    nfu = sum(len(v) for v in m.bfu)
+    nfd = sum(len(v) for v in m.bfd)
+
+    def lu(lo, hi, k):
+        return np.exp(rng.uniform(np.log(lo), np.log(hi), k))
+    alpha = lu(1e-14, 1e-10, nfu)
+    alpha[rng.random(nfu) < 0.1] = 1e6
+    sp = lu(1e-14, 1e-11, nfd)
+    sp[rng.random(nfd) < 0.1] = 0.0
+    den = lu(1e-12, 1.0, m.nlev)
+    den[rng.random(m.nlev) < 0.1] = 1e-14
+    return MatomCell(a21=lu(1e3, 1e9, nl), pesc=rng.uniform(1e-4, 1.0, nl), q21=lu(1e-12, 1e-7, nl),
+                     b12=lu(1e5, 1e12, nl), q12=lu(1e-14, 1e-8, nl), qrec=lu(1e-30, 1e-24, npht),
+                     qion=lu(1e-14, 1e-9, npht), jbar=lu(1e-20, 1e-12, nbu), gamma=lu(1e-4, 1e2, nfu), alpha_st=alpha,
+                     recomb_sp=sp, den=den, cool_bb=lu(1e-30, 1e-22, nl), cool_bf=lu(1e-30, 1e-22, npht),
+                     cool_bftot=float(lu(1e-25, 1e-21, 1)[0]), cool_adiabatic=float(lu(1e-28, 1e-23, 1)[0]),
+                     cool_ff=float(lu(1e-26, 1e-22, 1)[0]), cool_ff_lofreq=float(lu(1e-28, 1e-24, 1)[0]),
+                     t_e=float(10 ** rng.uniform(3.5, 5.5)), ne=float(10 ** rng.uniform(6, 12)))
+
+
+def matom_jump_inputs(m: MatomModel, cells, density_phot_min: float = 1e-10) -> dict:
+    """The arrays matom_rate_matrices_batched takes for a model and its cells:
+    per-level jump lists (starts and targets) and, cell after cell, one
+    coefficient per jump, computed as calc_matom_matrix computes them on the
+    host (a21 * p_escape, b12 * jbar, the density ratio, the k-packet to
+    r-packet sum in the routine's order)."""
+    nlev = m.nlev
+    lists = {"bbd": ([], []), "aug": ([], []), "bfd": ([], []), "bbu": ([], []), "bfu": ([], [])}
+    aug_rate = []
+    for u in range(nlev):
+        for key in lists:
+            lists[key][0].append(len(lists[key][1]))
+        lists["bbd"][1].extend(int(m.line_lo[i]) for i in m.bbd[u])
+        if m.aug_idx[u] >= 0:
+            a = int(m.aug_idx[u])
+            for k in range(int(m.n_aug[u])):
+                lists["aug"][1].append(int(m.aug_target[a][k]))
+                aug_rate.append(float(m.aug_A[a]) * float(m.aug_branch[a][k]))
+        lists["bfd"][1].extend(int(m.phot_lo[i]) for i in m.bfd[u])
+        lists["bbu"][1].extend(int(m.line_up[i]) for i in m.bbu[u])
+        lists["bfu"][1].extend(int(m.phot_up[i]) for i in m.bfu[u])
+    out = {"nlev": nlev, "ex": np.ascontiguousarray(m.ex, np.float64), "aug_rate": np.array(aug_rate, np.float64)}
+    for key, (st, tg) in lists.items():
+        out[key + "_start"] = np.array(st + [len(tg)], np.int32)
+        out[key + "_target"] = np.array(tg, np.int32)
+    mac_l = [i for i in range(m.line_lo.size) if m.line_macro[i]]
+    mac_p = [i for i in range(m.phot_lo.size) if m.phot_macro[i]]
+    out["kbb_target"] = np.array([int(m.line_up[i]) for i in mac_l], np.int32)
+    out["kbf_target"] = np.array([int(m.phot_up[i]) for i in mac_p], np.int32)
+    cols = {k: [] for k in ("bbd_rad", "bbd_coll", "bfd_sp", "bfd_qrec", "bbu_rad", "bbu_coll", "bfu_gamma",
+                            "bfu_alpha", "bfu_ratio", "bfu_qion", "kbb", "kbf", "kr", "ne")}
+    for c in cells:
+        ibu = ifu = ifd = 0
+        for u in range(nlev):
+            for i in m.bbd[u]:
+                cols["bbd_rad"].append(float(c.a21[i]) * float(c.pesc[i]))
+                cols["bbd_coll"].append(float(c.q21[i]))
+            for i in m.bfd[u]:
+                cols["bfd_sp"].append(float(c.recomb_sp[ifd]))
+                cols["bfd_qrec"].append(float(c.qrec[i]))
+                ifd += 1
+            for i in m.bbu[u]:
+                cols["bbu_rad"].append(float(c.b12[i]) * float(c.jbar[ibu]))
+                cols["bbu_coll"].append(float(c.q12[i]))
+                ibu += 1
+            for i in m.bfu[u]:
+                lo = float(c.den[m.phot_lo[i]])
+                cols["bfu_gamma"].append(float(c.gamma[ifu]))
+                cols["bfu_alpha"].append(float(c.alpha_st[ifu]))
+                cols["bfu_ratio"].append(float(c.den[m.phot_up[i]]) / lo if lo >= density_phot_min else 0.0)
+                cols["bfu_qion"].append(float(c.qion[i]))
+                ifu += 1
+        cols["kbb"].extend(float(c.cool_bb[i]) for i in mac_l)
+        cols["kbf"].extend(float(c.cool_bf[i]) for i in mac_p)
+        kr = 0.0
+        for i in range(m.line_lo.size):
+            if not m.line_macro[i]:
+                kr += float(c.cool_bb[i])
+        for i in range(m.phot_lo.size):
+            if not m.phot_macro[i]:
+                kr += float(c.cool_bf[i])
+        kr += c.cool_bftot
+        kr += c.cool_adiabatic
+        kr += c.cool_ff + c.cool_ff_lofreq
+        cols["kr"].append(kr)
+        cols["ne"].append(float(c.ne))
+    for k, v in cols.items():
+        out[k] = np.array(v, np.float64)
+    out["ncell"] = len(cells)
+    return out
