@@ -772,6 +772,123 @@ def run_sweep(args):
     return 0
 
 
+def run_rows(args):
+    """The rows around the batched solve, each through its public call on one
+    GPU, wall clock over --steps calls after --warmup (every call synchronises):
+    the macro-atom epilogue and draws on the config-1 batch, the GPU-assembled
+    ion lock-step, and both rate-matrix assemblies.  One JSON line."""
+    import ctypes
+
+    import torch
+
+    from python_b200 import engine
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+
+    def clock(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fn()
+        torch.cuda.synchronize(dev)
+        return (time.perf_counter() - t0) / args.steps
+
+    out = {"metric": "rows around the batched solve: throughput of each public call", "impl": "ours",
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic (seeded generators)"}
+    # macro-atom epilogue and draws: config-1 batch, device-resident
+    b = wl.config1(nsys=8192)
+    nsys = b.nsys
+    dn = np.ascontiguousarray(b.n, np.int32)
+    offv = (np.arange(nsys, dtype=np.int64) * 61)
+    dA = torch.from_numpy(b.A).to(dev)
+    dR = torch.rand(nsys * 61, dtype=torch.float64, device=dev)
+    dB = torch.empty_like(dA)
+    dC = torch.empty_like(dA)
+    dst = torch.empty(nsys, dtype=torch.int32, device=dev)
+    lib = engine.load()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def matom():
+        rc = lib.matom_matrices_batched(nsys, dn.ctypes.data, b.offA.ctypes.data, offv.ctypes.data, vp(dA), vp(dR),
+                                        vp(dB), vp(dC), vp(dst))
+        assert rc == 0, engine.last_error()
+    t_matom = clock(matom)
+    dX = torch.empty_like(dA)
+    plan = engine.Plan(b, engine.FP64)
+
+    def inv_only():
+        plan.execute(dA, dX, dst)
+        torch.cuda.synchronize(dev)
+    t_inv = clock(inv_only)
+    plan.close()
+    nq = 1 << 20
+    rng = np.random.default_rng(5)
+    sysi = torch.from_numpy(rng.integers(0, nsys, nq).astype(np.int32)).to(dev)
+    lvl = torch.from_numpy(rng.integers(0, 61, nq).astype(np.int32)).to(dev)
+    zz = torch.rand(nq, dtype=torch.float64, device=dev)
+    tgt = torch.empty(nq, dtype=torch.int32, device=dev)
+
+    def draws():
+        rc = lib.matom_sample_batched(nq, nsys, dn.ctypes.data, b.offA.ctypes.data, vp(dC), vp(sysi), vp(lvl), vp(zz),
+                                      vp(tgt))
+        assert rc == 0, engine.last_error()
+    t_draw = clock(draws)
+    out["matom_epilogue"] = {"workload": "8192 x n=61 inverse + B = N^-1 diag(R) + row running totals",
+                             "systems_per_s": nsys / t_matom, "ms": t_matom * 1e3, "inverse_alone_ms": t_inv * 1e3,
+                             "draws_per_s": nq / t_draw, "draws": nq}
+    del dA, dR, dB, dC, dX
+    # ion rate matrices: a 181-ion table (13 elements, H to Ni), 20,000 cells
+    tab = wl.ion_table(zs=(1, 2, 6, 7, 8, 10, 12, 14, 16, 18, 20, 26, 28), seed=21)
+    ncell = 20000
+    rates = wl.ion_rates(tab, ncell, seed=22)
+    ne = np.full(ncell, 1e10)
+    nh1, nh2 = np.full(ncell, 1e4), np.full(ncell, 1e10)
+    t_ion = clock(lambda: engine.ion_rate_matrices(tab, rates, ne, nh1, nh2))
+    blk = int((tab.elem_n.astype(np.int64) ** 2).sum())
+    out["ion_rate_matrices"] = {"workload": f"{ncell} cells x {tab.nions} ions ({tab.nelem} element blocks)",
+                                "cells_per_s": ncell / t_ion, "ms": t_ion * 1e3,
+                                "bytes_out": ncell * (blk + tab.nions) * 8,
+                                "note": "host arrays in and out: the call uploads the coefficients and returns A"}
+    # the lock-step with GPU assembly: 4096 cells of the 48-ion table
+    tab2 = wl.ion_table()
+    nc2 = 4096
+    rates2 = wl.ion_rates(tab2, nc2, seed=300)
+    rng = np.random.default_rng(301)
+    nh = np.exp(rng.uniform(np.log(1e6), np.log(1e12), nc2))
+    dens = nh[:, None] * np.array([1.0, 0.1, 3e-4, 5e-4, 3e-5])[None, :]
+    rounds = []
+
+    def lock():
+        den0 = np.zeros((nc2, tab2.nions))
+        den0[:, tab2.elem_first] = 1.0
+        ne0 = 0.1 * nh
+        st, it = engine.ion_populations_lockstep_rates(tab2, rates2, 0, dens, ne0, den0)
+        rounds.append(int(it.max()))
+    t_lock = clock(lock)
+    out["ion_lockstep_rates"] = {"workload": f"{nc2} cells x {tab2.nions} ions, n_e iteration to convergence",
+                                 "cells_per_s": nc2 / t_lock, "ms": t_lock * 1e3, "rounds": rounds[-1]}
+    # macro-atom jump matrices: 8192 cells of a 58-level model, device outputs
+    m = wl.matom_model()
+    cells = [wl.matom_cell(m, 7000 + c) for c in range(64)]
+    inp1 = wl.matom_jump_inputs(m, cells)
+    rep = 128                                   # 8192 cells: the 64 coefficient sets repeated
+    inp = dict(inp1)
+    for k in engine.MATOM_RATE_FIELDS:
+        inp[k] = np.tile(inp1[k], rep)
+    inp["ncell"] = 64 * rep
+    nr = m.nlev + 1
+    dN = torch.empty((inp["ncell"], nr, nr), dtype=torch.float64, device=dev)
+    dRr = torch.empty((inp["ncell"], nr), dtype=torch.float64, device=dev)
+    t_mq = clock(lambda: engine.matom_rate_matrices(inp, dN, dRr))
+    out["matom_rate_matrices"] = {"workload": f"{inp['ncell']} cells x {m.nlev} levels + k-packet",
+                                  "cells_per_s": inp["ncell"] / t_mq, "ms": t_mq * 1e3,
+                                  "note": "host coefficients in, N and R left on the device"}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -789,6 +906,8 @@ def main(argv=None):
                     help="skip timing the reference's cuSOLVER build")
     ap.add_argument("--cusolver-seconds", type=float, default=5.0)
     ap.add_argument("--ref-seconds", type=float, default=120.0)
+    ap.add_argument("--rows", action="store_true",
+                    help="time the rows around the batched solve (matom epilogue and draws, assemblies, lock-step)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args(argv)
@@ -796,6 +915,8 @@ def main(argv=None):
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.rows:
+        return run_rows(args)
     if args.config == 2:
         return run_sweep(args)
     return run_ours(args)

@@ -704,16 +704,33 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
   rc = c->get_plan(kInvert, nsys, n, offA, nullptr, SIROCCO_FP64, &p);
   if (rc) return rc;
   int64_t totV = 0;
-  for (int s = 0; s < nsys; ++s) totV = std::max<int64_t>(totV, offv[s] + n[s]);
+  int maxn = 0;
+  for (int s = 0; s < nsys; ++s) {
+    totV = std::max<int64_t>(totV, offv[s] + n[s]);
+    maxn = std::max(maxn, n[s]);
+  }
+  // blocks that fit 48 KB of shared memory are staged there (coalesced traffic)
+  const size_t tile_bytes = sizeof(double) * size_t(maxn) * size_t(maxn);
+  const bool tiled = tile_bytes <= size_t(48) << 10;
+  auto epilogue = [&](double* Bp, const double* Rp, double* Cp, const int* stp) -> int {
+    const int grid = std::max(1, std::min(nsys, p->num_sms * 16));
+    if (tiled)
+      matom_epilogue_tile_kernel<<<grid, 128, tile_bytes, c->stream>>>(nsys, p->d_n, p->d_offA,
+                                                                       static_cast<const int64_t*>(c->bOv.ptr), Bp,
+                                                                       Rp, Cp, stp);
+    else
+      matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA,
+                                                         static_cast<const int64_t*>(c->bOv.ptr), Bp, Rp, Cp, stp);
+    SS_CUDA(cudaGetLastError());
+    return 0;
+  };
   if ((rc = c->bOv.ensure(sizeof(int64_t) * size_t(nsys)))) return rc;
   int64_t* dOv = static_cast<int64_t*>(c->bOv.ptr);
   SS_CUDA(cudaMemcpyAsync(dOv, offv, sizeof(int64_t) * size_t(nsys), cudaMemcpyHostToDevice, c->stream));
-  const int grid = std::max(1, std::min(nsys, p->num_sms * 16));
   if (is_device_ptr(N)) {
     rc = plan_run(p, N, nullptr, B, status, nullptr, c->stream);
     if (rc) return rc;
-    matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA, dOv, B, R, C, status);
-    SS_CUDA(cudaGetLastError());
+    if ((rc = epilogue(B, R, C, status))) return rc;
     SS_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   }
@@ -730,8 +747,7 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
   SS_CUDA(cudaMemcpyAsync(dR, R, bytesV, cudaMemcpyHostToDevice, c->stream));
   rc = plan_run(p, dN, nullptr, dB, dst, nullptr, c->stream);
   if (rc) return rc;
-  matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA, dOv, dB, dR, dC, dst);
-  SS_CUDA(cudaGetLastError());
+  if ((rc = epilogue(dB, dR, dC, dst))) return rc;
   SS_CUDA(cudaMemcpyAsync(B, dB, bytesA, cudaMemcpyDeviceToHost, c->stream));
   if (C) SS_CUDA(cudaMemcpyAsync(C, dC, bytesA, cudaMemcpyDeviceToHost, c->stream));
   SS_CUDA(cudaMemcpyAsync(status, dst, sizeof(int) * size_t(nsys), cudaMemcpyDeviceToHost, c->stream));

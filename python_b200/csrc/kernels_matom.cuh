@@ -42,6 +42,47 @@ __global__ void __launch_bounds__(128) matom_epilogue_kernel(int nsys, const int
   }
 }
 
+// The same for systems whose n x n block fits the dynamic shared memory: the
+// block is scaled with coalesced loads and stores, staged in shared memory,
+// and each thread runs its row's running total there (the same additions in
+// the same order), after which the totals leave with coalesced stores.
+__global__ void __launch_bounds__(128) matom_epilogue_tile_kernel(int nsys, const int* __restrict__ n,
+                                                                  const int64_t* __restrict__ offA,
+                                                                  const int64_t* __restrict__ offv,
+                                                                  double* __restrict__ B,
+                                                                  const double* __restrict__ R,
+                                                                  double* __restrict__ C,
+                                                                  const int* __restrict__ status) {
+  extern __shared__ double tile[];   // [n][n] of the current system
+  for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+    const int ns = n[s];
+    const int nn = ns * ns;
+    const bool ok = status[s] == 0;
+    double* __restrict__ Bs = B + offA[s];
+    const double* __restrict__ Rs = R + offv[s];
+    for (int e = threadIdx.x; e < nn; e += blockDim.x) {
+      const int c = e % ns;
+      const double b = ok ? mul_rn(Bs[e], __ldg(Rs + c)) : 0.0;
+      Bs[e] = b;
+      tile[e] = b;
+    }
+    if (C) {
+      __syncthreads();
+      for (int r = threadIdx.x; r < ns; r += blockDim.x) {
+        double total = 0.0;
+        for (int c = 0; c < ns; ++c) {
+          total = add_rn(total, tile[r * ns + c]);
+          tile[r * ns + c] = total;
+        }
+      }
+      __syncthreads();
+      double* __restrict__ Cs = C + offA[s];
+      for (int e = threadIdx.x; e < nn; e += blockDim.x) Cs[e] = tile[e];
+    }
+    __syncthreads();
+  }
+}
+
 // Query i draws from row level[i] of system sys[i] with the number z[i]: the
 // reference returns 0 when z <= 0 and otherwise the first column whose running
 // total is not below z.  target[i] = -1 when the row total stays below z (the

@@ -116,3 +116,17 @@ def test_matom_device_pointers(engine):
     assert lib.matom_sample_batched(4096, batch.nsys, p(n), p(offA), d(dC), d(sys), d(level), d(z), d(tgt)) == 0
     want = engine.matom_sample(batch.n, batch.offA, C, sys.cpu().numpy(), level.cpu().numpy(), z.cpu().numpy())
     assert np.array_equal(tgt.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+def test_matom_matrices_tiled_blocks(engine):
+    # every block within 48 KB: the epilogue stages each system in shared memory
+    batch, R, offv = wl.matom_cells([61] * 40 + [1, 5, 33, 47, 78], seed=13)
+    B, C, st = engine.matom_matrices(batch, R, offv)
+    inv, sti = engine.invert_batched(batch)
+    np.testing.assert_array_equal(st, sti)
+    for s in range(batch.nsys):
+        n, o, v = int(batch.n[s]), int(batch.offA[s]), int(offv[s])
+        b = B[o:o + n * n].reshape(n, n)
+        assert np.array_equal(b, inv[o:o + n * n].reshape(n, n) * R[v:v + n][None, :]), s
+        assert np.array_equal(C[o:o + n * n].reshape(n, n), np.cumsum(b, axis=1)), s
