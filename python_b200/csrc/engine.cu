@@ -1344,9 +1344,15 @@ static int run_matom_rate_matrices(const sirocco_matom_table* t, int ncell, cons
   v.ncell = ncell;
   v.N = devN ? N : static_cast<double*>(c->bMN.ptr);
   v.R = devR ? R : static_cast<double*>(c->bMR.ptr);
-  const int64_t threads = int64_t(ncell) * nr;
-  matom_assemble_kernel<<<unsigned((threads + kMatomAsmThreads - 1) / kMatomAsmThreads), kMatomAsmThreads, 0,
-                          c->stream>>>(v);
+  // a block's rows are built in shared memory when at least a warp of them fits 48 KB
+  const size_t row_bytes = sizeof(double) * size_t(nr), smem_cap = size_t(48) << 10;
+  int bt = kMatomAsmThreads;
+  while (bt > 32 && size_t(bt) * row_bytes > smem_cap) bt -= 32;
+  const bool staged = size_t(bt) * row_bytes <= smem_cap;
+  if (!staged) bt = kMatomAsmThreads;
+  const int64_t rows = int64_t(ncell) * nr;
+  matom_assemble_kernel<<<unsigned((rows + bt - 1) / bt), bt, staged ? size_t(bt) * row_bytes : 0, c->stream>>>(
+      v, staged);
   SS_CUDA(cudaGetLastError());
   if (!devN) SS_CUDA(cudaMemcpyAsync(N, v.N, sizeof(double) * nc * nr * nr, cudaMemcpyDeviceToHost, c->stream));
   if (!devR) SS_CUDA(cudaMemcpyAsync(R, v.R, sizeof(double) * nc * nr, cudaMemcpyDeviceToHost, c->stream));

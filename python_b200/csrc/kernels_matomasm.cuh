@@ -3,10 +3,12 @@
 //
 // Row u of Q, R and the normalisation Q_norm come only from level u's own
 // jumps (the k-packet row from the macro lines' and continua's cooling
-// rates), so one thread builds one row: it zeroes its row of N, accumulates
-// every jump's contributions in the reference's order with one rounding per
-// product, sum and difference, and then writes N = I - Q / Q_norm and
-// R / Q_norm.  The row stays in the output buffer (L1/L2) while it is built.
+// rates), so one thread builds one row: it zeroes its row, accumulates every
+// jump's contributions in the reference's order with one rounding per
+// product, sum and difference, and then forms N = I - Q / Q_norm and
+// R / Q_norm.  The rows of a block are built in shared memory when they fit
+// (every += stays on chip) and leave with one coalesced copy: consecutive
+// threads own consecutive rows of N.  Larger models build them in place.
 #pragma once
 #include "ss_common.cuh"
 
@@ -26,15 +28,10 @@ struct MatomAsmView {
   double* R;   // [ncell][nlev + 1]
 };
 
-constexpr int kMatomAsmThreads = 128;
-
-__global__ void __launch_bounds__(kMatomAsmThreads) matom_assemble_kernel(MatomAsmView v) {
-  const int nr = v.nlev + 1, K = v.nlev;
-  const int64_t tid = int64_t(blockIdx.x) * kMatomAsmThreads + threadIdx.x;
-  if (tid >= int64_t(v.ncell) * nr) return;
-  const int cell = int(tid / nr), u = int(tid - int64_t(cell) * nr);
-  double* __restrict__ q = v.N + (int64_t(cell) * nr + u) * nr;
-  for (int t = 0; t < nr; ++t) q[t] = 0.0;
+// Row u of cell `cell` into q (zeroed): Q, then N = I - Q / Q_norm; R / Q_norm
+// to v.R.
+__device__ __forceinline__ void assemble_row(const MatomAsmView& v, int cell, int u, int nr, int K,
+                                             double* __restrict__ q) {
   double r = 0.0, qn = 0.0;
   const double ne = v.ne[cell];
   if (u < K) {
@@ -119,6 +116,29 @@ __global__ void __launch_bounds__(kMatomAsmThreads) matom_assemble_kernel(MatomA
     for (int t = 0; t < nr; ++t) q[t] = div_rn(-q[t], qn);
   q[u] = 1.0;
   v.R[int64_t(cell) * nr + u] = (qn > 0.0) ? div_rn(r, qn) : r;
+}
+
+constexpr int kMatomAsmThreads = 128;
+
+// staged: the block's rows live in dynamic shared memory ([blockDim][nlev + 1])
+__global__ void __launch_bounds__(kMatomAsmThreads) matom_assemble_kernel(MatomAsmView v, bool staged) {
+  extern __shared__ double srow[];
+  const int nr = v.nlev + 1, K = v.nlev;
+  const int64_t nrows = int64_t(v.ncell) * nr;
+  const int64_t row0 = int64_t(blockIdx.x) * blockDim.x;
+  const int64_t tid = row0 + threadIdx.x;
+  if (tid < nrows) {
+    const int cell = int(tid / nr), u = int(tid - int64_t(cell) * nr);
+    double* __restrict__ q = staged ? srow + int64_t(threadIdx.x) * nr : v.N + tid * nr;
+    for (int t = 0; t < nr; ++t) q[t] = 0.0;
+    assemble_row(v, cell, u, nr, K, q);
+  }
+  if (staged) {
+    __syncthreads();
+    const int64_t nb = min(int64_t(blockDim.x), nrows - row0) * nr;
+    double* __restrict__ dst = v.N + row0 * nr;
+    for (int64_t e = threadIdx.x; e < nb; e += blockDim.x) dst[e] = srow[e];
+  }
 }
 
 }  // namespace ss

@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("levels,seed,ncell", [((12, 20, 16, 9, 1), 7, 24), ((6, 30, 25, 4, 1), 99, 12),
-                                               ((3, 2, 1), 5, 8)])
+                                               ((3, 2, 1), 5, 8),
+                                               ((60, 80, 60, 1), 3, 3)])   # 201 levels: rows built in place
 def test_assembly_matches_restatement(levels, seed, ncell):
     m = wl.matom_model(ion_levels=levels, seed=seed)
     cells = [wl.matom_cell(m, 1000 * seed + c) for c in range(ncell)]
