@@ -1185,17 +1185,32 @@ static int run_ion_lockstep_rates(const sirocco_ion_table* t, int ncell, const s
   int64_t blkA = 0;
   if ((rc = ion_asm_prepare(t, ncell, r, c, v, elem_of, blkA))) return rc;
   const int nions = t->nions, nelem = t->nelem;
-  std::vector<int> n;
+  std::vector<int> n, pc;
   std::vector<int64_t> offA, offv;
+  std::vector<double> pne, ph1, ph2;
   auto round = [&](int na, const int* cells, const double* nea, const double* nh1, const double* nh2, double* x,
                    int* st) -> int {
-    int rc2 = ion_asm_round(c, v, na, cells, nea, nh1, nh2);
+    // The active set shrinks round by round; padded to a power of two with
+    // repeats of its first cell (their results are dropped) it takes at most
+    // log2(ncell) + 1 layouts, whose plans stay cached.  Every system is solved
+    // on its own, so the padding changes no result.
+    int np2 = 1;
+    while (np2 < na) np2 <<= 1;
+    pc.assign(cells, cells + na);
+    pne.assign(nea, nea + na);
+    ph1.assign(nh1, nh1 + na);
+    ph2.assign(nh2, nh2 + na);
+    pc.resize(np2, cells[0]);
+    pne.resize(np2, nea[0]);
+    ph1.resize(np2, nh1[0]);
+    ph2.resize(np2, nh2[0]);
+    int rc2 = ion_asm_round(c, v, np2, pc.data(), pne.data(), ph1.data(), ph2.data());
     if (rc2) return rc2;
-    if ((rc2 = c->bIX.ensure(sizeof(double) * size_t(na) * nions)) ||
-        (rc2 = c->bISt.ensure(sizeof(int) * size_t(na) * nelem)))
+    if ((rc2 = c->bIX.ensure(sizeof(double) * size_t(np2) * nions)) ||
+        (rc2 = c->bISt.ensure(sizeof(int) * size_t(np2) * nelem)))
       return rc2;
-    ion_block_layout(na, nions, nelem, t->elem_first, t->elem_n, blkA, n, offA, offv);
-    rc2 = run_batched(kSolve, na * nelem, n.data(), offA.data(), v.A, offv.data(), v.b,
+    ion_block_layout(np2, nions, nelem, t->elem_first, t->elem_n, blkA, n, offA, offv);
+    rc2 = run_batched(kSolve, np2 * nelem, n.data(), offA.data(), v.A, offv.data(), v.b,
                       static_cast<double*>(c->bIX.ptr), static_cast<int*>(c->bISt.ptr), c->mode);
     if (rc2) return rc2;
     SS_CUDA(cudaMemcpy(x, c->bIX.ptr, sizeof(double) * size_t(na) * nions, cudaMemcpyDeviceToHost));
