@@ -15,7 +15,7 @@ pytestmark = pytest.mark.skipif(not oracle.ion_reference_available(),
 
 def _cases():
     yield wl.ion_table(), 6
-    yield wl.ion_table(zs=(1, 2, 7, 10, 14, 26), seed=11), 4
+    yield wl.ion_table(zs=(1, 2, 7, 10, 14, 26, 30), seed=11), 4   # Zn: a 31-ion block
     t = wl.ion_table(zs=(1, 6, 8), seed=12)          # no charge-exchange entries at all
     t.cx_nion1 = t.cx_nion1[:0]
     t.cx_nion2 = t.cx_nion2[:0]
