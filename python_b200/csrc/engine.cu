@@ -1050,6 +1050,8 @@ static int ion_asm_prepare(const sirocco_ion_table* t, int ncell, const sirocco_
           return SIROCCO_EINVAL;
         }
     }
+  // the table is valid: from here on the device is needed
+  if ((rc = c->init())) return rc;
   // ints: elem_first, elem_n, ion_z, ion_istate, flags, cx_start, cx_idx, in_start, in_idx, in_yield
   std::vector<int> ints;
   std::vector<size_t> io;
@@ -1154,8 +1156,7 @@ static int run_ion_rate_matrices(const sirocco_ion_table* t, int ncell, const si
     return SIROCCO_EINVAL;
   }
   Context* c = ctx();
-  int rc = c->init();
-  if (rc) return rc;
+  int rc;
   IonAsmView v;
   std::vector<int> elem_of;
   int64_t blkA = 0;
@@ -1178,8 +1179,7 @@ static int run_ion_lockstep_rates(const sirocco_ion_table* t, int ncell, const s
     return SIROCCO_EINVAL;
   }
   Context* c = ctx();
-  int rc = c->init();
-  if (rc) return rc;
+  int rc;
   IonAsmView v;
   std::vector<int> elem_of;
   int64_t blkA = 0;

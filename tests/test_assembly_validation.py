@@ -26,3 +26,30 @@ def test_malformed_tables_are_rejected(key, bad):
     with pytest.raises(engine.EngineError):
         engine.matom_rate_matrices(inp)
     assert engine.last_error()
+
+
+def _ion_case(kind):
+    tab = wl.ion_table()
+    rates = wl.ion_rates(tab, 2)
+    if kind == "cxr_neutral":
+        rates.cxr[1, int(tab.elem_first[2])] = 1e-9          # lands in another element's block
+    elif kind == "cx_last_ion":
+        last = int(tab.elem_first[3] + tab.elem_n[3] - 1)
+        tab.cx_nion1 = np.append(tab.cx_nion1, np.int32(last))
+        tab.cx_nion2 = np.append(tab.cx_nion2, np.int32(1))   # against H II
+        rates = wl.ion_rates(tab, 2)
+    elif kind == "yield_row":
+        tab.inner_yield = tab.inner_yield.copy()
+        tab.inner_yield[0] = len(tab.yield_prob)              # no such row
+    elif kind == "overlap":
+        tab.elem_first = tab.elem_first.copy()
+        tab.elem_first[1] = 1                                 # He starts inside H
+    return tab, rates
+
+
+@pytest.mark.parametrize("kind", ["cxr_neutral", "cx_last_ion", "yield_row", "overlap"])
+def test_malformed_ion_tables_are_rejected(kind):
+    tab, rates = _ion_case(kind)
+    with pytest.raises(engine.EngineError):
+        engine.ion_rate_matrices(tab, rates, np.ones(2), np.ones(2), np.ones(2))
+    assert engine.last_error()
