@@ -64,6 +64,15 @@ int gpu_invert_matrix(double *matrix, double *inverse, int num_rows);
 #define SIROCCO_MIXED 1  /* equilibrated FP32 factorisation + FP64 refinement,
                             exact FP64 for any system whose result or code the
                             refinement cannot vouch for                          */
+#define SIROCCO_FAST 2   /* inverses of certified matrices -- nonsingular
+                            M-matrices: positive diagonal, off-diagonal entries
+                            <= 0, every row strictly dominant by a relative
+                            margin of at least 1e-5, as the macro-atom jumping
+                            matrix N = I - Q/Q_norm is wherever every level can
+                            deactivate -- by FP64 Gauss-Jordan without pivoting
+                            (code 0, as GSL's, and within ~1e-11 of GSL's
+                            inverse); every other system, and every solve, by
+                            the GSL-exact FP64 path of SIROCCO_FP64             */
 
 /* Library error codes returned by the batched entry points (per-system codes
    go to status[]); positive values are CUDA error codes. */
@@ -83,7 +92,13 @@ int gpu_invert_matrix(double *matrix, double *inverse, int num_rows);
 int solve_matrix_batched(int nsys, const int *n, const int64_t *offA, const double *A,
                          const int64_t *offv, const double *b, double *x, int *status);
 
-/* Batched inverse, called once per cycle from the matom-matrix cell loop. */
+/* Batched inverse, called once per cycle from the matom-matrix cell loop.
+   status[s] is invert_matrix's code: 0, 1 (an exact zero pivot in GSL's LU) or
+   21 (GSL_ESING: an infinite pivot, which LU_invx turns into a zero on the
+   diagonal of U^-1), the output left untouched for 1 and 21.  In SIROCCO_FAST
+   mode a system may also get -3: the certified kernel's staging copy did not
+   arrive within its bounded wait (about a second), so the system was not
+   processed; no correct run produces it. */
 int invert_matrix_batched(int nsys, const int *n, const int64_t *offA, const double *A,
                           double *Ainv, int *status);
 

@@ -47,6 +47,10 @@
    (gsl_errno.h: GSL_EDOM = 1). */
 #define ORACLE_GSL_EDOM 1
 
+/* GSL_ESING (gsl_errno.h: 21), returned by gsl_linalg_tri_invert when the
+   triangle it is given has an exact zero on its diagonal (invtri.c:233-245). */
+#define ORACLE_GSL_ESING 21
+
 /* First index of the strict maximum of |a[i*n+j]| over i in [j, n), scanning
    from max = 0.0 like cblas idamax (cblas/source_iamax_r.h): NaNs are never
    chosen and an all-zero column returns j. */
@@ -276,8 +280,12 @@ unit_lower_inverse (double *l, int n)
 }
 
 /* matrix_cpu.c:224 cpu_invert_matrix -> lu.c:415 gsl_linalg_LU_invert.
-   Returns 0, or GSL_EDOM (1) when U has an exact zero on its diagonal, in which
-   case inv is left untouched as in the reference. */
+   Returns 0, or GSL_EDOM (1) when U has an exact zero on its diagonal, or
+   GSL_ESING (21) when U has an infinite one, in which cases inv is left
+   untouched as in the reference.  The second code comes from the order of
+   LU_invx (lu.c:458-463): U is inverted in place first, which leaves 1/u_ii on
+   the diagonal, and gsl_linalg_tri_invert then checks that diagonal for exact
+   zeros before it inverts the unit lower triangle; 1/(+-Inf) is zero. */
 int
 oracle_invert_matrix (double *a, double *inv, int n)
 {
@@ -293,6 +301,13 @@ oracle_invert_matrix (double *a, double *inv, int n)
     free (perm);
     return ORACLE_GSL_EDOM;
   }
+  for (int i = 0; i < n; i++)
+    if (1.0 / a[(size_t) i * n + i] == 0.0)
+    {
+      free (ipiv);
+      free (perm);
+      return ORACLE_GSL_ESING;
+    }
   double *w = (double *) malloc (nn * sizeof (double));
   double *x = (double *) malloc (nn * sizeof (double));
   memcpy (w, a, nn * sizeof (double));

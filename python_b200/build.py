@@ -45,7 +45,9 @@ def build_engine(force: bool = False, verbose: bool = False) -> Path:
 
 def build_oracle(reference: bool = True) -> None:
     targets = ["port"]
-    ref_tree = Path(os.environ.get("SIROCCO_REFERENCE", "/root/reference"))
+    # the reference checkout: SIROCCO_REFERENCE, else a `reference` directory
+    # beside this repository's root; without it only the restatement is built
+    ref_tree = Path(os.environ.get("SIROCCO_REFERENCE", str(ROOT.parent / "reference")))
     if reference and (ref_tree / "source" / "matrix_cpu.c").exists():
         targets.append("ref")
         if (ref_tree / "source" / "matrix_ion.c").exists():

@@ -2,8 +2,12 @@
 //
 // A plan groups the systems of one batch layout into size buckets, each served
 // by one kernel family (kernels_small.cuh for n <= 32, kernels_cta.cuh for
-// n <= 256, kernels_global.cuh above), keeps the layout on the device, and
-// launches the buckets on forked streams so small and large systems overlap.
+// n <= 1024; kernels_cert.cuh for the certified inverses of SIROCCO_FAST mode),
+// keeps the layout on the device, and launches the buckets on forked streams so
+// small and large systems overlap.  A plan with certified buckets runs in two
+// phases: the certified kernels first, which append every system that fails
+// the certificate to a device-side list per exact size class, then the
+// GSL-exact kernels over those lists.
 // The drop-in entry points (solve_matrix, invert_matrix) and the host-pointer
 // batched calls run through a per-thread context that caches plans and
 // grow-only device staging buffers.
@@ -24,6 +28,7 @@
 #include <vector>
 
 #include "../../include/sirocco_solve.h"
+#include "kernels_cert.cuh"
 #include "kernels_cta.cuh"
 #include "kernels_global.cuh"
 #include "kernels_ionasm.cuh"
@@ -56,7 +61,7 @@ static void set_error(const char* fmt, ...) {
   } while (0)
 
 // ---------------------------------------------------------------- kernels --
-enum Family : int { kFamSmall = 0, kFamCta = 1, kFamGlobal = 2 };
+enum Family : int { kFamSmall = 0, kFamCta = 1, kFamGlobal = 2, kFamCgj = 3 };
 
 struct KernelSpec {
   const void* fn = nullptr;
@@ -65,6 +70,8 @@ struct KernelSpec {
   int sys_per_block = 1;
   int blocks_per_sm = 1;
   int64_t work_slab = 0;   // CTA family with the matrix in global memory: doubles per CTA
+  int cluster = 1;         // CTAs per system (certified family above order 128)
+  int max_ctas = 0;        // CTAs resident on the whole GPU at once
 };
 
 // size classes of the small family (padded row length NP, lanes per system G)
@@ -77,6 +84,16 @@ static const int kCtaP[] = {
 };
 constexpr int kCtaClasses = int(sizeof(kCtaP) / sizeof(kCtaP[0]));
 
+// padded orders of the certified Gauss-Jordan classes (cgj_classes.inc)
+static const int kCgjP[] = {
+#define SS_CGJ_CLASS(I, P, RT, CT, CL, MINB) P,
+#include "cgj_classes.inc"
+#undef SS_CGJ_CLASS
+};
+constexpr int kCgjClasses = int(sizeof(kCgjP) / sizeof(kCgjP[0]));
+// below this order the warp-group kernels of the exact path are faster
+constexpr int kCgjMinN = 33;
+
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
     if (n <= kSmallNP[i]) return i;
@@ -85,6 +102,12 @@ static int small_class(int n) {
 static int cta_class(int n) {
   for (int i = 0; i < kCtaClasses; ++i)
     if (n <= kCtaP[i]) return i;
+  return -1;
+}
+static int cgj_class(int n) {
+  if (n < kCgjMinN) return -1;
+  for (int i = 0; i < kCgjClasses; ++i)
+    if (n <= kCgjP[i]) return i;
   return -1;
 }
 
@@ -137,6 +160,25 @@ static KernelSpec cta_spec(int cls) {
   return k;
 }
 
+static KernelSpec cgj_spec(int cls) {
+  KernelSpec k;
+#define SS_CGJ_CLASS(I, P, RT, CT, CL, MINB)                                         \
+  case I: {                                                                          \
+    using Sh = CgjShape<P, RT, CT, CL, MINB>;                                        \
+    k.fn = reinterpret_cast<const void*>(&cgj_inverse_kernel<P, RT, CT, CL, MINB>);  \
+    k.threads = Sh::NTH;                                                             \
+    k.dyn_smem = Sh::dyn_smem;                                                       \
+    k.cluster = CL;                                                                  \
+    break;                                                                           \
+  }
+  switch (cls) {
+#include "cgj_classes.inc"
+    default: break;
+  }
+#undef SS_CGJ_CLASS
+  return k;
+}
+
 template <int KIND>
 static KernelSpec global_spec(int nmax) {
   KernelSpec k;
@@ -161,6 +203,31 @@ static int finish_spec(KernelSpec& k) {
     return SIROCCO_ESIZE;
   }
   k.blocks_per_sm = nb;
+  int dev = 0, sms = 0;
+  SS_CUDA(cudaGetDevice(&dev));
+  SS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  k.max_ctas = nb * sms;
+  if (k.cluster > 1) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = unsigned(k.cluster);
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(unsigned(k.cluster * sms));
+    cfg.blockDim = dim3(unsigned(k.threads));
+    cfg.dynamicSmemBytes = k.dyn_smem;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    SS_CUDA(cudaOccupancyMaxActiveClusters(&ncl, k.fn, &cfg));
+    if (ncl < 1) {
+      set_error("a cluster of %d CTAs (threads %d, shared %zu) cannot be scheduled", k.cluster, k.threads,
+                k.dyn_smem);
+      return SIROCCO_ESIZE;
+    }
+    k.max_ctas = ncl * k.cluster;
+  }
   return 0;
 }
 
@@ -174,6 +241,8 @@ struct Bucket {
   int grid;
   int64_t slab;   // scratch elements per CTA (global solves, CTA classes in global memory)
   int64_t scratch_off;
+  int phase;      // 1: certified kernels and directly listed systems; 2: fallback lists
+  int fb;         // phase 2: index of the fallback list this launch serves
 };
 
 }  // namespace ss
@@ -193,6 +262,13 @@ struct sirocco_plan {
   double* d_scratch = nullptr;
   int64_t scratch_elems = 0;   // workspace doubles the buckets need
   bool own_scratch = true;     // false: d_scratch points into a pipeline's shared workspace
+  // certified inverses: per system, the fallback list of its exact size class
+  int nfb = 0;                 // fallback lists (exact classes that certified systems belong to)
+  std::vector<int> fb_off;     // start of each list in d_fblist
+  int* d_xcls = nullptr;
+  int* d_fboff = nullptr;
+  int* d_fblist = nullptr;
+  int* d_fbcount = nullptr;
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
   cudaEvent_t ev_fork = nullptr;
@@ -206,11 +282,56 @@ static void plan_free(sirocco_plan* p) {
   cudaFree(p->d_offA);
   cudaFree(p->d_offv);
   cudaFree(p->d_list);
+  cudaFree(p->d_xcls);
+  cudaFree(p->d_fboff);
+  cudaFree(p->d_fblist);
+  cudaFree(p->d_fbcount);
   if (p->own_scratch) cudaFree(p->d_scratch);
   for (auto s : p->side) cudaStreamDestroy(s);
   for (auto e : p->ev) cudaEventDestroy(e);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   delete p;
+}
+
+// Host-side check of a batch layout, before anything touches the device: every
+// order in 1..SIROCCO_MAX_N, every offset non-negative, and no two systems'
+// output ranges overlapping (the inverse of system s is written at offA[s], a
+// solution at offv[s]; matrices of a solve are only read and may share
+// storage).  Packed layouts, whose offsets increase, are checked in one pass;
+// others are sorted first.
+static int check_layout(int kind, int nsys, const int* n, const int64_t* offA, const int64_t* offv) {
+  if (nsys < 0 || (nsys > 0 && (!n || !offA || (kind == kSolve && !offv)))) {
+    set_error("invalid layout arguments");
+    return SIROCCO_EINVAL;
+  }
+  for (int s = 0; s < nsys; ++s) {
+    if (n[s] < 1 || n[s] > SIROCCO_MAX_N) {
+      set_error("system %d has order %d (supported 1..%d)", s, n[s], SIROCCO_MAX_N);
+      return n[s] < 1 ? SIROCCO_EINVAL : SIROCCO_ESIZE;
+    }
+    if (offA[s] < 0 || (kind == kSolve && offv[s] < 0)) {
+      set_error("system %d has a negative offset", s);
+      return SIROCCO_EINVAL;
+    }
+  }
+  const int64_t* off = (kind == kSolve) ? offv : offA;
+  auto len = [&](int s) { return (kind == kSolve) ? int64_t(n[s]) : int64_t(n[s]) * n[s]; };
+  bool sorted = true;
+  for (int s = 0; s + 1 < nsys && sorted; ++s) sorted = off[s] <= off[s + 1];
+  std::vector<int> order;
+  if (!sorted) {
+    order.resize(nsys);
+    for (int s = 0; s < nsys; ++s) order[s] = s;
+    std::sort(order.begin(), order.end(), [&](int x, int y) { return off[x] < off[y]; });
+  }
+  for (int i = 0; i + 1 < nsys; ++i) {
+    const int a = sorted ? i : order[i], b = sorted ? i + 1 : order[i + 1];
+    if (off[a] + len(a) > off[b]) {
+      set_error("the %s of systems %d and %d overlap", kind == kSolve ? "solutions" : "inverses", a, b);
+      return SIROCCO_EINVAL;
+    }
+  }
+  return 0;
 }
 
 static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, const int64_t* offA,
@@ -224,10 +345,11 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
     set_error("kind must be 0 (solve) or 1 (invert)");
     return SIROCCO_EINVAL;
   }
-  if (mode != SIROCCO_FP64 && mode != SIROCCO_MIXED) {
+  if (mode != SIROCCO_FP64 && mode != SIROCCO_MIXED && mode != SIROCCO_FAST) {
     set_error("unknown precision mode %d", mode);
     return SIROCCO_EMODE;
   }
+  if (int rc = check_layout(kind, nsys, n, offA, offv)) return rc;
   std::unique_ptr<sirocco_plan, void (*)(sirocco_plan*)> p(new sirocco_plan(), plan_free);
   p->kind = kind;
   p->mode = mode;
@@ -235,8 +357,12 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   SS_CUDA(cudaGetDevice(&p->device));
   SS_CUDA(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device));
 
-  // bucket the systems: key = (family, class); global family sorted by size
-  std::vector<int> small_l[8], cta_l[kCtaClasses], glob_l;
+  // bucket the systems: key = (family, class); global family sorted by size.
+  // Certified inverses (SIROCCO_FAST) go to the Gauss-Jordan classes; each also
+  // has a place in the fallback list of its exact class (small or CTA family).
+  const bool cert = (kind == kInvert && mode == SIROCCO_FAST);
+  std::vector<int> small_l[8], cta_l[kCtaClasses], glob_l, cgj_l[kCgjClasses];
+  int small_fb[8] = {}, cta_fb[kCtaClasses] = {};
   for (int s = 0; s < nsys; ++s) {
     const int ns = n[s];
     if (ns < 1 || ns > SIROCCO_MAX_N) {
@@ -246,9 +372,39 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
     p->totA = std::max<int64_t>(p->totA, offA[s] + int64_t(ns) * ns);
     if (kind == kSolve) p->totV = std::max<int64_t>(p->totV, offv[s] + ns);
     int c;
+    if (cert && (c = cgj_class(ns)) >= 0) {
+      cgj_l[c].push_back(s);
+      int e;
+      if ((e = small_class(ns)) >= 0) small_fb[e]++;
+      else cta_fb[cta_class(ns)]++;
+      continue;
+    }
     if ((c = small_class(ns)) >= 0) small_l[c].push_back(s);
     else if ((c = cta_class(ns)) >= 0) cta_l[c].push_back(s);
     else glob_l.push_back(s);
+  }
+  // fallback lists: one per exact class that certified systems belong to
+  int small_fbi[8], cta_fbi[kCtaClasses];
+  std::vector<int> xcls;
+  if (cert) {
+    int off = 0;
+    auto add_fb = [&](int cnt) {
+      if (cnt == 0) return -1;
+      p->fb_off.push_back(off);
+      off += cnt;
+      return p->nfb++;
+    };
+    for (int e = 0; e < 8; ++e) small_fbi[e] = add_fb(small_fb[e]);
+    for (int e = 0; e < kCtaClasses; ++e) cta_fbi[e] = add_fb(cta_fb[e]);
+    if (p->nfb > 0) {
+      xcls.assign(nsys, -1);
+      for (int c = 0; c < kCgjClasses; ++c)
+        for (int s : cgj_l[c]) {
+          const int e = small_class(n[s]);
+          xcls[s] = (e >= 0) ? small_fbi[e] : cta_fbi[cta_class(n[s])];
+        }
+      p->fb_off.push_back(off);   // total size of the lists
+    }
   }
   // largest systems first within the global bucket (longest jobs start first)
   std::stable_sort(glob_l.begin(), glob_l.end(), [&](int x, int y) { return n[x] > n[y]; });
@@ -256,21 +412,26 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   std::vector<int> list;
   list.reserve(nsys);
   int64_t scratch_elems = 0;
-  auto add_bucket = [&](Family fam, int cls, const std::vector<int>& l) -> int {
-    if (l.empty()) return 0;
+  // a bucket serves either systems of the plan's list (count of them) or, in
+  // phase 2, fallback list fb (at most count entries, filled on the device)
+  auto add_bucket_n = [&](Family fam, int cls, const std::vector<int>* l, int fb, int cnt) -> int {
+    if (cnt == 0) return 0;
     Bucket b{};
     b.fam = fam;
     b.cls = cls;
-    b.count = int(l.size());
+    b.count = cnt;
+    b.phase = (fb >= 0) ? 2 : 1;
+    b.fb = fb;
     b.list_off = int(list.size());
-    list.insert(list.end(), l.begin(), l.end());
-    if (fam == kFamSmall) b.spec = (kind == kSolve) ? small_spec<kSolve>(cls, mode) : small_spec<kInvert>(cls, mode);
+    if (l) list.insert(list.end(), l->begin(), l->end());
+    if (fam == kFamCgj) b.spec = cgj_spec(cls);
+    else if (fam == kFamSmall) b.spec = (kind == kSolve) ? small_spec<kSolve>(cls, mode) : small_spec<kInvert>(cls, mode);
     else if (fam == kFamCta) b.spec = (kind == kSolve) ? cta_spec<kSolve>(cls) : cta_spec<kInvert>(cls);
     else b.spec = (kind == kSolve) ? global_spec<kSolve>(cls) : global_spec<kInvert>(cls);
     int rc = finish_spec(b.spec);
     if (rc) return rc;
     const int blocks_needed = (b.count + b.spec.sys_per_block - 1) / b.spec.sys_per_block;
-    b.grid = std::max(1, std::min(blocks_needed, b.spec.blocks_per_sm * p->num_sms));
+    b.grid = std::max(1, std::min(blocks_needed * b.spec.cluster, b.spec.max_ctas));
     if (fam == kFamGlobal && kind == kSolve) {
       b.slab = (int64_t(cls) * cls + 31) / 32 * 32;
       b.scratch_off = scratch_elems;
@@ -284,12 +445,23 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
     p->buckets.push_back(b);
     return 0;
   };
+  auto add_bucket = [&](Family fam, int cls, const std::vector<int>& l) -> int {
+    return add_bucket_n(fam, cls, &l, -1, int(l.size()));
+  };
   int rc = 0;
   if (!glob_l.empty() && (rc = add_bucket(kFamGlobal, n[glob_l.front()], glob_l))) return rc;
+  for (int c = kCgjClasses - 1; c >= 0; --c)
+    if ((rc = add_bucket(kFamCgj, c, cgj_l[c]))) return rc;
   for (int c = kCtaClasses - 1; c >= 0; --c)
     if ((rc = add_bucket(kFamCta, c, cta_l[c]))) return rc;
   for (int c = 7; c >= 0; --c)
     if ((rc = add_bucket(kFamSmall, c, small_l[c]))) return rc;
+  if (cert) {
+    for (int c = kCtaClasses - 1; c >= 0; --c)
+      if (cta_fbi[c] >= 0 && (rc = add_bucket_n(kFamCta, c, nullptr, cta_fbi[c], cta_fb[c]))) return rc;
+    for (int c = 7; c >= 0; --c)
+      if (small_fbi[c] >= 0 && (rc = add_bucket_n(kFamSmall, c, nullptr, small_fbi[c], small_fb[c]))) return rc;
+  }
 
   if (nsys > 0) {
     SS_CUDA(cudaMalloc(&p->d_n, sizeof(int) * nsys));
@@ -302,12 +474,23 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
       SS_CUDA(cudaMalloc(&p->d_offv, sizeof(int64_t) * nsys));
       SS_CUDA(cudaMemcpy(p->d_offv, offv, sizeof(int64_t) * nsys, cudaMemcpyHostToDevice));
     }
+    if (p->nfb > 0) {
+      SS_CUDA(cudaMalloc(&p->d_xcls, sizeof(int) * nsys));
+      SS_CUDA(cudaMemcpy(p->d_xcls, xcls.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice));
+      SS_CUDA(cudaMalloc(&p->d_fboff, sizeof(int) * p->fb_off.size()));
+      SS_CUDA(cudaMemcpy(p->d_fboff, p->fb_off.data(), sizeof(int) * p->fb_off.size(), cudaMemcpyHostToDevice));
+      SS_CUDA(cudaMalloc(&p->d_fblist, sizeof(int) * std::max(1, p->fb_off.back())));
+      SS_CUDA(cudaMalloc(&p->d_fbcount, sizeof(int) * p->nfb));
+      SS_CUDA(cudaMemset(p->d_fbcount, 0, sizeof(int) * p->nfb));
+    }
   }
   p->scratch_elems = scratch_elems;
   p->own_scratch = alloc_scratch;
   if (alloc_scratch && scratch_elems > 0) SS_CUDA(cudaMalloc(&p->d_scratch, sizeof(double) * scratch_elems));
-  // one side stream per bucket beyond the first
-  for (size_t i = 1; i < p->buckets.size(); ++i) {
+  // one side stream per bucket of a phase beyond the first
+  size_t per_phase[3] = {0, 0, 0};
+  for (auto& b : p->buckets) per_phase[b.phase]++;
+  for (size_t i = 1; i < std::max(per_phase[1], per_phase[2]); ++i) {
     cudaStream_t st;
     SS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     p->side.push_back(st);
@@ -333,7 +516,27 @@ static int launch_bucket(const sirocco_plan* p, const Bucket& b, const double* A
   v.diag = diag;
   v.list = p->d_list + b.list_off;
   v.count = b.count;
-  if (b.fam == kFamGlobal) {
+  if (b.fb >= 0) {
+    v.list = p->d_fblist + p->fb_off[b.fb];
+    v.count_dev = p->d_fbcount + b.fb;
+  }
+  if (b.fam == kFamCgj) {
+    CertArgs ca{p->d_xcls, p->d_fboff, p->d_fblist, p->d_fbcount};
+    void* args[] = {&v, &ca};
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = unsigned(b.spec.cluster);
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(unsigned(b.grid));
+    cfg.blockDim = dim3(unsigned(b.spec.threads));
+    cfg.dynamicSmemBytes = b.spec.dyn_smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = b.spec.cluster > 1 ? 1 : 0;
+    SS_CUDA(cudaLaunchKernelExC(&cfg, b.spec.fn, args));
+  } else if (b.fam == kFamGlobal) {
     int nmax = b.cls;
     double* scratch = p->d_scratch ? p->d_scratch + b.scratch_off : nullptr;
     int64_t slab = b.slab;
@@ -354,21 +557,34 @@ static int launch_bucket(const sirocco_plan* p, const Bucket& b, const double* A
   return 0;
 }
 
-static int plan_run(sirocco_plan* p, const double* A, const double* bvec, double* out, int* status,
-                    int* diag, cudaStream_t st) {
-  if (p->buckets.empty()) return 0;
-  if (p->buckets.size() == 1) return launch_bucket(p, p->buckets[0], A, bvec, out, status, diag, st);
+// The buckets of one phase, forked onto the side streams and joined back into st.
+static int run_phase(sirocco_plan* p, int phase, const double* A, const double* bvec, double* out, int* status,
+                     int* diag, cudaStream_t st) {
+  std::vector<const Bucket*> bs;
+  for (auto& b : p->buckets)
+    if (b.phase == phase) bs.push_back(&b);
+  if (bs.empty()) return 0;
+  if (bs.size() == 1) return launch_bucket(p, *bs[0], A, bvec, out, status, diag, st);
   SS_CUDA(cudaEventRecord(p->ev_fork, st));
-  for (size_t i = 1; i < p->buckets.size(); ++i) SS_CUDA(cudaStreamWaitEvent(p->side[i - 1], p->ev_fork, 0));
-  int rc = launch_bucket(p, p->buckets[0], A, bvec, out, status, diag, st);
+  for (size_t i = 1; i < bs.size(); ++i) SS_CUDA(cudaStreamWaitEvent(p->side[i - 1], p->ev_fork, 0));
+  int rc = launch_bucket(p, *bs[0], A, bvec, out, status, diag, st);
   if (rc) return rc;
-  for (size_t i = 1; i < p->buckets.size(); ++i) {
-    rc = launch_bucket(p, p->buckets[i], A, bvec, out, status, diag, p->side[i - 1]);
+  for (size_t i = 1; i < bs.size(); ++i) {
+    rc = launch_bucket(p, *bs[i], A, bvec, out, status, diag, p->side[i - 1]);
     if (rc) return rc;
     SS_CUDA(cudaEventRecord(p->ev[i - 1], p->side[i - 1]));
   }
-  for (size_t i = 1; i < p->buckets.size(); ++i) SS_CUDA(cudaStreamWaitEvent(st, p->ev[i - 1], 0));
+  for (size_t i = 1; i < bs.size(); ++i) SS_CUDA(cudaStreamWaitEvent(st, p->ev[i - 1], 0));
   return 0;
+}
+
+static int plan_run(sirocco_plan* p, const double* A, const double* bvec, double* out, int* status,
+                    int* diag, cudaStream_t st) {
+  if (p->buckets.empty()) return 0;
+  if (p->nfb > 0) SS_CUDA(cudaMemsetAsync(p->d_fbcount, 0, sizeof(int) * size_t(p->nfb), st));
+  int rc = run_phase(p, 1, A, bvec, out, status, diag, st);
+  if (rc) return rc;
+  return run_phase(p, 2, A, bvec, out, status, diag, st);
 }
 
 // -------------------------------------------------------- per-thread context --
@@ -615,6 +831,7 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
     set_error("invalid batched arguments");
     return SIROCCO_EINVAL;
   }
+  if (int rc = check_layout(kind, nsys, n, offA, offv)) return rc;
   Context* c = ctx();
   int rc = c->init();
   if (rc) return rc;
@@ -697,6 +914,12 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
     set_error("invalid macro-atom arguments");
     return SIROCCO_EINVAL;
   }
+  if (int rc = check_layout(kInvert, nsys, n, offA, nullptr)) return rc;
+  for (int s = 0; s < nsys; ++s)
+    if (offv[s] < 0) {
+      set_error("cell %d has a negative offset of its deactivation rates", s);
+      return SIROCCO_EINVAL;
+    }
   Context* c = ctx();
   int rc = c->init();
   if (rc) return rc;
@@ -1522,29 +1745,37 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlabs * kNoAll
 
 constexpr int kMaxDevices = 64;
 static std::mutex g_noalloc_mu;
-static double* g_noalloc_ptr[kMaxDevices] = {};
+static bool g_noalloc_ready[kMaxDevices] = {};
 
 // The array's device address on the current device.  In host code the symbol
-// g_noalloc_scratch is only a host-side handle, so the address is looked up once
-// per device with that device current, then reused.
-static int noalloc_scratch(double** out) {
+// g_noalloc_scratch is only a host-side handle, so the address is looked up with
+// that device current, on every call (the lookup is cheap, and a cached address
+// would go stale if the caller reset the device).  The first call on a device
+// also raises the kernel's shared-memory limit to what the largest allowed
+// order needs, once, so that concurrent calls with different orders never see
+// a limit below their launch.
+static int noalloc_scratch(double** out, const void* fn) {
   int dev = 0;
   SS_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("device %d beyond the %d devices the no-allocation path tracks", dev, kMaxDevices);
     return SIROCCO_EINVAL;
   }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      set_error("cudaGetSymbolAddress of the no-allocation scratch failed: %s", cudaGetErrorString(e));
-      return int(e);
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ready[dev]) {
+      SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(global_smem_bytes(kNoAllocMaxN))));
+      g_noalloc_ready[dev] = true;
     }
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
   }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    set_error("cudaGetSymbolAddress of the no-allocation scratch failed: %s", cudaGetErrorString(e));
+    return int(e);
+  }
+  *out = static_cast<double*>(p);
   return 0;
 }
 
@@ -1625,7 +1856,7 @@ int invert_matrix_batched(int nsys, const int* n, const int64_t* offA, const dou
 }
 
 int sirocco_set_precision(int mode) {
-  if (mode != SIROCCO_FP64 && mode != SIROCCO_MIXED) {
+  if (mode != SIROCCO_FP64 && mode != SIROCCO_MIXED && mode != SIROCCO_FAST) {
     set_error("unknown precision mode %d", mode);
     return SIROCCO_EMODE;
   }
@@ -1711,13 +1942,12 @@ int solve_matrix_batched_noalloc(int nsys, int nmax, const int* n, const int64_t
               nmax, kNoAllocMaxN);
     return SIROCCO_ESIZE;
   }
-  double* scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
-  if (rc) return rc;
   static_assert(global_panel_width(kNoAllocMaxN) == 16, "no-allocation path uses the 16-wide panel");
   const void* fn = reinterpret_cast<const void*>(&global_exact_kernel<kSolve, 16, true>);
+  double* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch, fn);
+  if (rc) return rc;
   const size_t smem = global_smem_bytes(nmax);
-  SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   BatchView v;
   v.n = n;
   v.offA = offA;

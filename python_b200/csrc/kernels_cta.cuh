@@ -102,14 +102,15 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
   double* pivbuf = dsm + Sh::off_pb;       // [B+1] pivot row and its reciprocal (PW > 1)
   int* ps_s = reinterpret_cast<int*>(dsm + Sh::n_dbl);   // [P] position of each row
   int* perm = ps_s + P;                    // [P] row at each position
-  int* flags = perm + P;                   // [0] singular
+  int* flags = perm + P;                   // [0] singular, [1] an infinite pivot
   unsigned* cand = reinterpret_cast<unsigned*>(flags + 4);   // [PW][4] per-warp pivot candidates
 
   const int t = threadIdx.x;
   const int wid = t >> 5, wl = t & 31;
   const int tc = t % Sh::TGC, tr = t / Sh::TGC;
 
-  for (int item = blockIdx.x; item < bv.count; item += gridDim.x) {
+  const int count = batch_count(bv);
+  for (int item = blockIdx.x; item < count; item += gridDim.x) {
     const int s = bv.list[item];
     const int n = bv.n[s];
     const double* __restrict__ Ag = bv.A + bv.offA[s];
@@ -128,7 +129,10 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
       }
     }
     for (int r = t; r < P; r += NT) { ps_s[r] = r; perm[r] = r; }
-    if (t == 0) flags[0] = 0;
+    if (t == 0) {
+      flags[0] = 0;
+      flags[1] = 0;
+    }
     if (!GM) cp_async_wait_all();
     __syncthreads();
 
@@ -269,6 +273,7 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
           }
           const double ujj = pv[0];
           if (__any_sync(FULL, ujj == 0.0)) { sing = true; break; }
+          if (KIND == kInvert && t == 0 && isinf(ujj)) flags[1] = 1;
           double lrow[RPL];
 #pragma unroll
           for (int i = 0; i < RPL; ++i) lrow[i] = mul_rn(pr[i][0], rinv);
@@ -542,9 +547,11 @@ cta_exact_kernel(BatchView bv, double* __restrict__ work) {
       __syncthreads();
     }
 
-    if (singular) {
+    if (singular || (KIND == kInvert && flags[1])) {
+      // a zero pivot: GSL_EDOM; for an inverse, an infinite one: GSL_ESING
+      // (LU_invx finds 1/u_jj = 0 after inverting U); the output is untouched
       if (t == 0) {
-        bv.status[s] = (KIND == kSolve) ? kSolveSingular : kInvertSingular;
+        bv.status[s] = (KIND == kSolve) ? kSolveSingular : (singular ? kInvertSingular : kInvertInfPivot);
         if (bv.diag) bv.diag[s] = kDiagExact;
       }
       __syncthreads();

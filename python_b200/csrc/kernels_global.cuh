@@ -61,7 +61,8 @@ global_exact_kernel(BatchView bv, int nmax, double* scratch, int64_t slab) {
   const int wid = t >> 5, wl = t & 31;
   const int tr = t >> 4, tc = t & 15;                 // 16 x 16 thread grid of the update
 
-  for (int item = blockIdx.x; item < bv.count; item += gridDim.x) {
+  const int count = batch_count(bv);
+  for (int item = blockIdx.x; item < count; item += gridDim.x) {
     const int s = DIRECT ? item : bv.list[item];
     const int n = bv.n[s];
     if (DIRECT && (n < 1 || n > nmax)) {

@@ -51,7 +51,8 @@ small_mixed_solve_kernel(BatchView bv, MixedParams mp) {
   const unsigned gmask = group_mask<G>();
   SmallSmem<NP>& sm = smem_all[grp];
 
-  for (int item = blockIdx.x * GPB + grp; item < bv.count; item += gridDim.x * GPB) {
+  const int count = batch_count(bv);
+  for (int item = blockIdx.x * GPB + grp; item < count; item += gridDim.x * GPB) {
     const int s = bv.list[item];
     const int n = bv.n[s];
     const int64_t ov = bv.offv[s];

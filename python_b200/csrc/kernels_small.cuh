@@ -74,10 +74,11 @@ __device__ __forceinline__ void small_stage(SmallSmem<NP>& sm, const double* __r
 // row held in a[].  Returns true when U has an exact zero on its diagonal.
 template <int KIND, int NP, int G>
 __device__ __forceinline__ bool small_exact_factor(SmallSmem<NP>& sm, double (&a)[NP], int n, int lane,
-                                                   unsigned gmask, int& pos) {
+                                                   unsigned gmask, int& pos, bool& inf_piv) {
   const bool act = lane < n;
   bool done = false;
   bool sing = false;
+  inf_piv = false;
   pos = lane;
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
@@ -110,6 +111,7 @@ __device__ __forceinline__ bool small_exact_factor(SmallSmem<NP>& sm, double (&a
       }
       __syncwarp(gmask);
       const double ujj = sm.piv[j];
+      inf_piv |= isinf(ujj);
       if (ujj == 0.0) {
         sing = true;   // lu.c:540 singular(): the result is decided
       } else {
@@ -193,7 +195,8 @@ __device__ __forceinline__ int small_exact_solve(SmallSmem<NP>& sm, const double
 #pragma unroll
   for (int k = 0; k < NP; ++k) a[k] = (act && k < n) ? sm.stage[lane * S + k] : 0.0;
   int pos;
-  if (small_exact_factor<kSolve, NP, G>(sm, a, n, lane, gmask, pos)) return kSolveSingular;
+  bool inf_piv;
+  if (small_exact_factor<kSolve, NP, G>(sm, a, n, lane, gmask, pos, inf_piv)) return kSolveSingular;
   if (act) sm.lop[pos] = lane;
   double t = act ? bg[lane] : 0.0;   // (P b) at this row's position
   __syncwarp(gmask);
@@ -243,7 +246,8 @@ small_exact_kernel(BatchView bv) {
   const unsigned gmask = group_mask<G>();
   SmallSmem<NP>& sm = smem_all[grp];
 
-  for (int item = blockIdx.x * GPB + grp; item < bv.count; item += gridDim.x * GPB) {
+  const int count = batch_count(bv);
+  for (int item = blockIdx.x * GPB + grp; item < count; item += gridDim.x * GPB) {
     const int s = bv.list[item];
     const int n = bv.n[s];
     small_stage<NP, G>(sm, bv.A + bv.offA[s], n, lane, gmask);
@@ -261,8 +265,12 @@ small_exact_kernel(BatchView bv) {
 #pragma unroll
       for (int k = 0; k < NP; ++k) a[k] = (act && k < n) ? sm.stage[lane * S + k] : 0.0;
       int pos;
-      const bool sing = small_exact_factor<kInvert, NP, G>(sm, a, n, lane, gmask, pos);
-      if (!sing) {
+      bool inf_piv;
+      const bool sing = small_exact_factor<kInvert, NP, G>(sm, a, n, lane, gmask, pos, inf_piv);
+      // GSL's LU_invx inverts U in place and then finds 1/u_jj = 0 on the
+      // diagonal for an infinite pivot: GSL_ESING, output untouched
+      const int code = sing ? kInvertSingular : (inf_piv ? kInvertInfPivot : kOk);
+      if (code == kOk) {
         // rows of W by position, then the reverse-order column unscramble
         if (act) {
 #pragma unroll
@@ -288,7 +296,7 @@ small_exact_kernel(BatchView bv) {
         }
       }
       if (lane == 0) {
-        bv.status[s] = sing ? kInvertSingular : kOk;
+        bv.status[s] = code;
         if (bv.diag) bv.diag[s] = kDiagExact;
       }
     }

@@ -28,6 +28,16 @@ constexpr int kResidRel = 2;
 constexpr int kResidAbs = 3;
 constexpr int kSolveSingular = 4;
 constexpr int kInvertSingular = 1;
+// GSL_ESING: invert_matrix's code when U has an infinite pivot.  LU_invx
+// (lu.c:458-463) inverts U in place, leaving 1/u_jj = 0 on the diagonal, and
+// gsl_linalg_tri_invert refuses the unit lower triangle for that zero
+// (invtri.c:233-245).  The output is left untouched.
+constexpr int kInvertInfPivot = 21;
+// Engine status (not a reference code): a kernel's bounded wait for its own
+// staging copy ran out, so the system was not processed.  No correct run
+// produces it; it exists so that a stalled copy ends the kernel instead of
+// hanging the GPU.
+constexpr int kStageTimeout = -3;
 
 // residual threshold of cpu_solve_matrix (reference source/python.h:98)
 constexpr double kResidEps = 1.0e-6;
@@ -54,7 +64,15 @@ struct BatchView {
   int* diag;              // [nsys] diagnostic bits, may be null
   const int* list;        // systems of this bucket, indices into the batch
   int count;              // number of systems in list
+  const int* count_dev = nullptr;   // if set, the number of systems in list is read here
+                                    // (a list filled on the device by an earlier launch)
 };
+
+// Number of systems a launch serves: the device-side count when the list was
+// filled on the device, else the host-side count.
+__device__ __forceinline__ int batch_count(const BatchView& bv) {
+  return bv.count_dev ? *bv.count_dev : bv.count;
+}
 
 // Mixed-precision tuning (per launch).
 struct MixedParams {

@@ -18,6 +18,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libsirocco_solve.so"
 
 FP64 = 0
 MIXED = 1
+FAST = 2
 SOLVE = 0
 INVERT = 1
 

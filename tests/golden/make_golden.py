@@ -30,7 +30,9 @@ sys.path.insert(0, str(ROOT))
 from oracle import oracle  # noqa: E402
 from python_b200 import workloads as wl  # noqa: E402
 
-REF = Path(os.environ.get("SIROCCO_REFERENCE", "/root/reference"))
+# the reference checkout: SIROCCO_REFERENCE, else a `reference` directory beside
+# this repository's root
+REF = Path(os.environ.get("SIROCCO_REFERENCE", str(ROOT.parent / "reference")))
 FIX = REF / "source" / "tests" / "test_data" / "matrix"
 
 
@@ -147,5 +149,42 @@ def main() -> None:
     print("invert cases:", ib.nsys, "codes", np.bincount(si, minlength=2))
 
 
+def nonfinite_cases(rng):
+    """Macro-atom and dense matrices with one +Inf, -Inf or NaN entry, and a few
+    with several: the reference's invert_matrix returns 21 (GSL_ESING) where an
+    infinite value reaches the diagonal of U, 1 for an exact zero pivot, else 0;
+    its solve_matrix returns 4 or 0 and leaves the residual test to NaN."""
+    mats = []
+    for n in (2, 3, 5, 9, 17, 24, 31, 33, 48, 61, 65, 70):
+        for k in range(6):
+            m = wl.macro_matrix(rng, n) if k % 2 == 0 else rng.standard_normal((n, n))
+            i, j = rng.integers(0, n, 2)
+            m[i, j] = (np.inf, -np.inf, np.nan)[k % 3]
+            if k == 5 and n > 3:
+                m[rng.integers(n), rng.integers(n)] = np.inf
+                m[rng.integers(n)] = 0.0
+            mats.append(m)
+    return mats
+
+
+def main_nonfinite() -> None:
+    rng = np.random.default_rng(wl.BASE_SEED + 101)
+    mats = nonfinite_cases(rng)
+    ib = wl.from_matrices("invert", mats)
+    inv, si = oracle.invert(ib, "ref")
+    sb = wl.from_matrices("solve", mats, [rng.standard_normal(m.shape[0]) for m in mats])
+    xs, ss = oracle.solve(sb, "ref")
+    np.savez_compressed(HERE / "nonfinite_cases.npz", n=ib.n, offA=ib.offA, A=ib.A, inv_ref=inv,
+                        inv_status_ref=si, offv=sb.offv, b=sb.b, x_ref=xs, solve_status_ref=ss)
+    print("non-finite cases:", ib.nsys, "invert codes", np.unique(si, return_counts=True),
+          "solve codes", np.unique(ss, return_counts=True))
+
+
 if __name__ == "__main__":
-    main()
+    # python tests/golden/make_golden.py [--only nonfinite]
+    if sys.argv[1:] == ["--only", "nonfinite"]:
+        oracle.build_port()
+        main_nonfinite()
+    else:
+        main()
+        main_nonfinite()

@@ -1,0 +1,169 @@
+"""Certified inverses (SIROCCO_FAST) against the reference's GSL inverse.
+
+Matrices that pass the certificate (nonsingular M-matrices with a relative
+row-dominance margin of at least 1e-5) are inverted by Gauss-Jordan without
+pivoting: code 0, as GSL's, and the inverse within 1e-10 (max-abs, relative to
+the largest entry) of the reference build's.  Every other matrix falls back to
+the GSL-exact path, whose results must equal SIROCCO_FP64 mode's bit for bit.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from python_b200 import workloads as wl
+from tests.helpers import inverse_rel_err, same_values
+
+pytestmark = pytest.mark.gpu
+
+INV_TOL = 1e-10
+CERTIFIED_DIAG = 0
+
+
+def ref_invert(batch):
+    which = "ref" if oracle.available("ref") else "port"
+    return oracle.invert(batch, which, threads=oracle.host_threads())
+
+
+def run_plan(engine, batch, mode):
+    import torch
+    dev = torch.device("cuda")
+    A = torch.from_numpy(batch.A).to(dev)
+    out = torch.full_like(A, float("nan"))
+    st = torch.full((batch.nsys,), -99, dtype=torch.int32, device=dev)
+    diag = torch.full((batch.nsys,), -1, dtype=torch.int32, device=dev)
+    plan = engine.Plan(batch, mode)
+    plan.execute(A, out, st, diag=diag)
+    torch.cuda.synchronize()
+    plan.close()
+    return out.cpu().numpy(), st.cpu().numpy(), diag.cpu().numpy()
+
+
+def per_system_err(inv, ref, batch):
+    return np.array([inverse_rel_err(inv, ref, batch.n[s:s + 1], batch.offA[s:s + 1]) for s in range(batch.nsys)])
+
+
+def test_certified_config1_sample_matches_gsl(engine):
+    batch = wl.config1(nsys=2048)
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    assert (diag == CERTIFIED_DIAG).all(), "every config-1 matrix is an M-matrix with margin >= 1e-4"
+    assert inverse_rel_err(inv, ir, batch.n, batch.offA) <= INV_TOL
+
+
+@pytest.mark.parametrize("lo,hi", [(33, 64), (65, 128), (129, 192), (193, 256)])
+def test_certified_every_class_matches_gsl(engine, lo, hi):
+    rng = np.random.default_rng(lo)
+    sizes = list(range(lo, hi + 1, 3)) + [lo, hi]
+    batch = wl.macro_batch(sizes, seed=int(rng.integers(1 << 30)))
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    assert (diag == CERTIFIED_DIAG).all()
+    err = per_system_err(inv, ir, batch)
+    assert err.max() <= INV_TOL, (batch.n[np.argmax(err)], err.max())
+
+
+def test_certified_config3_macro_sample(engine):
+    rng = np.random.default_rng(3)
+    batch = wl.macro_batch(rng.integers(20, 201, 400), seed=33)
+    inv, st, _ = run_plan(engine, batch, engine.FAST)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    assert per_system_err(inv, ir, batch).max() <= INV_TOL
+
+
+def uncertified_matrices(rng):
+    """Matrices that must fail the certificate, with the reason."""
+    out = []
+    m = wl.macro_matrix(rng, 40)
+    m[5, :] = 0.0
+    m[5, 5] = 1.0
+    m[5, 7] = -1.0                              # a level that cannot deactivate: margin 0
+    out.append(m)
+    m = wl.macro_matrix(rng, 70)
+    m[3, 9] = 1e-3                              # a positive off-diagonal entry
+    out.append(m)
+    m = wl.macro_matrix(rng, 100)
+    m[10, 11] = np.nan                          # non-finite entry
+    out.append(m)
+    m = wl.macro_matrix(rng, 33)
+    m[2, :] = 0.0                               # singular: the reference returns 1
+    out.append(m)
+    m = wl.macro_matrix(rng, 150)
+    m[0, 0] = 1.0 - 1e-6 + m[0, 0] - 1.0        # diagonal shrunk below the margin
+    m[0, 1:] = 0.0
+    m[0, 1] = -(1.0 - 2e-6)
+    out.append(m)
+    out.append(np.random.default_rng(1).standard_normal((60, 60)))   # general dense
+    m = wl.macro_matrix(rng, 200)
+    m[199, 198] = np.inf
+    out.append(m)
+    return out
+
+
+def test_uncertified_fall_back_to_the_exact_path(engine):
+    rng = np.random.default_rng(11)
+    bad = uncertified_matrices(rng)
+    good = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 257, 40)]
+    mats = good[:20] + bad + good[20:]
+    batch = wl.from_matrices("invert", mats)
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    inv64, st64, _ = run_plan(engine, batch, engine.FP64)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    np.testing.assert_array_equal(st, st64)
+    fb = (diag & (1 << 8)) != 0
+    nbad = len(bad)
+    assert fb[20:20 + nbad].all(), diag[20:20 + nbad]
+    assert not fb[:20].any() and not fb[20 + nbad:].any()
+    for s in np.nonzero(fb)[0]:
+        o, k = int(batch.offA[s]), int(batch.n[s])
+        if st[s] == 0:
+            assert same_values(inv[o:o + k * k], inv64[o:o + k * k]).all(), s
+    ok = st == 0
+    good_idx = np.array([s for s in range(batch.nsys) if not fb[s]])
+    sub_err = per_system_err(inv, ir, batch)
+    assert sub_err[good_idx].max() <= INV_TOL
+    assert ok[good_idx].all()
+
+
+def test_certified_plan_in_a_cuda_graph(engine):
+    import torch
+    rng = np.random.default_rng(5)
+    mats = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 257, 300)]
+    bad = uncertified_matrices(rng)
+    batch = wl.from_matrices("invert", mats[:150] + bad + mats[150:])
+    want, wst, _ = run_plan(engine, batch, engine.FAST)
+    dev = torch.device("cuda")
+    A = torch.from_numpy(batch.A).to(dev)
+    out = torch.zeros_like(A)
+    st = torch.full((batch.nsys,), -99, dtype=torch.int32, device=dev)
+    plan = engine.Plan(batch, engine.FAST)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        plan.execute(A, out, st, stream=s)   # warm-up outside the capture
+        s.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            plan.execute(A, out, st, stream=s)
+    for _ in range(2):
+        out.zero_()
+        st.fill_(-99)
+        g.replay()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        np.testing.assert_array_equal(st.cpu().numpy(), wst)
+        ok = np.repeat(wst == 0, batch.n.astype(np.int64) ** 2)
+        assert same_values(got[ok], want[ok]).all()
+    plan.close()
+
+
+def test_certified_host_batched_entry(engine):
+    """invert_matrix_batched in SIROCCO_FAST mode through host buffers, including
+    the chunked host pipeline (a batch above 32 MiB)."""
+    batch = wl.config1(nsys=1400)
+    inv, st = engine.invert_batched(batch, engine.FAST)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    assert inverse_rel_err(inv, ir, batch.n, batch.offA) <= INV_TOL

@@ -205,3 +205,59 @@ def test_mixed_well_conditioned_sets_accept_and_match(engine):
     check_mixed(engine, macro, require_accept=0.5)
     dense = wl.dense_batch("solve", rng.integers(2, 33, 600), seed=78)
     check_mixed(engine, dense, require_accept=0.3)
+
+
+# ------------------------------------------------------------ non-finite ----
+@pytest.mark.parametrize("mode", ["FP64", "FAST"])
+def test_nonfinite_codes_match_reference(engine, mode):
+    """Matrices with +Inf, -Inf or NaN entries: invert_matrix's codes, 21
+    (GSL_ESING, an infinite pivot) included, and solve_matrix's codes equal the
+    reference build's (tests/golden/nonfinite_cases.npz); a system whose code is
+    not 0 leaves its output untouched through the drop-in call."""
+    from tests.conftest import GOLDEN
+    g = dict(np.load(GOLDEN / "nonfinite_cases.npz"))
+    m = getattr(engine, mode)
+    ib = wl.Batch("invert", g["n"].astype(np.int32), g["offA"], g["A"])
+    _, si = engine.invert_batched(ib, m)
+    np.testing.assert_array_equal(si, g["inv_status_ref"])
+    sb = wl.Batch("solve", g["n"].astype(np.int32), g["offA"], g["A"], g["offv"], g["b"])
+    _, ss = engine.solve_batched(sb, m)
+    np.testing.assert_array_equal(ss, g["solve_status_ref"])
+    for s in np.nonzero(g["inv_status_ref"] == 21)[0][:4]:
+        code, inv = engine.invert_matrix(ib.matrix(int(s)).copy(), np.full((ib.n[s], ib.n[s]), 7.0))
+        assert code == 21 and (inv == 7.0).all()
+
+
+# --------------------------------------------------- drop-in CUDA names ----
+def test_gpu_named_entry_points_match_oracle(engine, golden_solve, golden_invert):
+    """gpu_solve_matrix / gpu_invert_matrix, the names of the reference's CUDA
+    build (source/matrix_gpu.h:20-21), on the golden cases: codes equal, solves
+    bit for bit, inverses to rounding."""
+    import ctypes
+    lib = engine.load()
+    dp = ctypes.POINTER(ctypes.c_double)
+    sb = batch_from_golden(golden_solve, "solve")
+    for s in range(0, sb.nsys, 7):
+        n = int(sb.n[s])
+        a = sb.matrix(s).copy()
+        b = sb.rhs(s).copy()
+        x = np.full(n, 7.0)
+        code = lib.gpu_solve_matrix(a.ctypes.data_as(dp), b.ctypes.data_as(dp), n, x.ctypes.data_as(dp))
+        assert code == golden_solve["status_ref"][s]
+        xr = golden_solve["x_ref"][sb.offv[s]:sb.offv[s] + n]
+        if code != 4:
+            assert same_values(x, xr).all(), s
+        else:
+            assert (x == 7.0).all()
+    ib = batch_from_golden(golden_invert, "invert")
+    for s in range(0, ib.nsys, 5):
+        n = int(ib.n[s])
+        m = ib.matrix(s).copy()
+        out = np.full((n, n), 7.0)
+        code = lib.gpu_invert_matrix(m.ctypes.data_as(dp), out.ctypes.data_as(dp), n)
+        assert code == golden_invert["status_ref"][s]
+        if code == 0:
+            r = golden_invert["inv_ref"][ib.offA[s]:ib.offA[s] + n * n].reshape(n, n)
+            assert np.max(np.abs(out - r)) <= 1e-10 * np.max(np.abs(r)), s
+        else:
+            assert (out == 7.0).all()

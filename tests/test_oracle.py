@@ -5,6 +5,7 @@ import pytest
 
 from oracle import oracle
 from python_b200 import workloads as wl
+from tests.conftest import GOLDEN
 from tests.helpers import batch_from_golden, inverse_rel_err, same_values
 
 
@@ -89,3 +90,18 @@ def test_live_reference_configs():
 def test_error_strings_match_reference_wording():
     assert oracle.error_string(2) == "some matrix rows failing relative error check"
     assert oracle.error_string(4).startswith("Unsolvable matrix!")
+
+
+def test_nonfinite_codes_match_reference_golden():
+    """Non-finite entries: the restatement returns the reference's codes, 21
+    (GSL_ESING) included, which LU_invx raises when an infinite value reaches
+    the diagonal of U (tests/golden/nonfinite_cases.npz, made by the reference
+    build)."""
+    g = dict(np.load(GOLDEN / "nonfinite_cases.npz"))
+    ib = wl.Batch("invert", g["n"].astype(np.int32), g["offA"], g["A"])
+    _, si = oracle.invert(ib, "port")
+    np.testing.assert_array_equal(si, g["inv_status_ref"])
+    assert 21 in set(si.tolist()) and 1 in set(si.tolist())
+    sb = wl.Batch("solve", g["n"].astype(np.int32), g["offA"], g["A"], g["offv"], g["b"])
+    _, ss = oracle.solve(sb, "port")
+    np.testing.assert_array_equal(ss, g["solve_status_ref"])

@@ -91,3 +91,26 @@ def test_noalloc_rejects_orders_beyond_its_scratch(engine):
     b = wl.dense_batch("solve", [40, 80], seed=4)
     rc, _, st = _noalloc(engine, b, 40)
     assert rc == 0 and st[0] == 0 and st[1] == -1
+
+
+def test_noalloc_full_size_systems_share_slabs(engine):
+    # at the largest order the static array holds 8 slabs, so 20 systems of
+    # order 512 run on 8 CTAs that each reuse one slab for several systems
+    b = wl.dense_batch("solve", [MAX_N] * 20, seed=21, log_spread=2.0)
+    xr, sr = _reference(engine, b)
+    for _ in range(2):
+        rc, x, st = _noalloc(engine, b, MAX_N)
+        assert rc == 0, engine.last_error()
+        np.testing.assert_array_equal(st, sr)
+        assert same_values(x, xr).all()
+
+
+def test_noalloc_matches_the_oracle(engine):
+    from oracle import oracle
+    b = _batch(13)
+    rc, x, st = _noalloc(engine, b, int(b.n.max()))
+    assert rc == 0, engine.last_error()
+    xo, so = oracle.solve(b, "port", threads=oracle.host_threads())
+    np.testing.assert_array_equal(st, so)
+    keep = np.repeat(so != 4, b.n)
+    assert same_values(x[keep], xo[keep]).all()
