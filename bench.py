@@ -3,8 +3,13 @@
 
 One step = every system of the workload solved / inverted once, inputs already
 resident in HBM (``value``), and the same through the C ABI with pinned host
-buffers, host<->device copies included (``e2e``).  Default workload: 8,192
-macro-atom jumping matrices of order 61 inverted (invert_matrix).
+buffers, host<->device copies included (``e2e``).  Default workload: the
+50k-cell mixed batch (per cell 10 ion-balance solves of orders 2-27 and one
+macro-atom inverse of order 20-200), the configuration the headline target is
+quoted on.  ``value`` runs the engine's certified mode (SIROCCO_FAST: macro-atom
+inverses that pass the M-matrix certificate by Gauss-Jordan without pivoting,
+everything else GSL-exact); ``plain_fp64_value`` is the same step with every
+system on the GSL-exact FP64 path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config 0|1|3|4]
     python bench.py --impl reference ...   # the reference's CPU path, all host cores
@@ -45,15 +50,22 @@ L2_BYTES = 126 * 2 ** 20
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 HBM_FALLBACK_GBS = 6650.0
 
-# DRAM traffic of the dominant kernel from the committed ncu captures, as a
-# ratio to its algorithmic bytes (captures of a smaller case are scaled by the
-# systems processed): {config: (size class, traffic / algorithmic bytes, capture)}
-TRAFFIC = {
-    1: ("cta64", 435.6 / 487.7, "profiles/cta_exact_kernel_inverse_8192x61.md"),
-    0: ("small28", 25.0 / 25.66, "profiles/small_exact_kernel_solve_4096x27.md"),
-    3: ("cta192", 2242.1 / 248.6, "profiles/cta_exact_kernel_inverse_n161-192_workspace.md"),
-    4: ("cta1024", 49803.5 / 373.7, "profiles/cta_exact_kernel_inverse_n897-1024_workspace.md"),
-}
+# DRAM traffic of the dominant kernel: the committed ncu summaries in
+# profiles/ carry a machine-readable line
+#     traffic-ratio: <size class> <DRAM bytes / algorithmic bytes> <workload>
+# for the capture they summarise; the bench scales it to the timed launch and
+# names the file it came from.
+PROFILES = ROOT / "profiles"
+
+
+def traffic_ratio(size_class_name: str):
+    for f in sorted(PROFILES.glob("*.md")):
+        for line in f.read_text().splitlines():
+            parts = line.strip().strip("`").split()
+            if len(parts) >= 3 and parts[0] == "traffic-ratio:" and parts[1] == size_class_name:
+                return float(parts[2]), f"profiles/{f.name}"
+    return None, None
+
 
 WORKLOADS = {
     0: "ion-balance solve, 4096 x n=27 (config-0 generator)",
@@ -80,8 +92,15 @@ def make_batches(config: int, nsys: int | None = None):
     raise SystemExit(f"unknown config {config}")
 
 
-def size_class(n: int) -> str:
+CGJ_P = (40, 48, 56, 64, 80, 96, 112, 128, 144, 160, 192, 224, 256)   # csrc/cgj_classes.inc
+
+
+def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:
     """Mirror of the engine's bucketing (python_b200/csrc/engine.cu)."""
+    if kind == "invert" and mode == "fast" and n >= 33:
+        for p in CGJ_P:
+            if n <= p:
+                return f"cgj{p}"
     for np_ in (4, 8, 12, 16, 20, 24, 28, 32):
         if n <= np_:
             return f"small{np_}"
@@ -92,6 +111,8 @@ def size_class(n: int) -> str:
 
 
 def kernel_name(kind: str, cls: str, mode: str) -> str:
+    if cls.startswith("cgj"):
+        return "cgj_inverse_kernel"
     if cls.startswith("small"):
         return ("small_mixed_solve_kernel" if (mode == "mixed" and kind == "solve") else "small_exact_kernel")
     return "cta_exact_kernel" if cls.startswith("cta") else "global_exact_kernel"
@@ -337,13 +358,15 @@ def fp64_peak_tflops(device) -> float:
 
 
 def accuracy(batch, out_np, status_np, mode, sample=512, seed=1):
-    """Error of the timed outputs against the CPU oracle on a sample."""
+    """Error of the timed outputs against the reference's GSL build (oracle/_ref,
+    else the restatement) on a sample."""
     from oracle import oracle
+    which = "ref" if oracle.available("ref") else "port"
     rng = np.random.default_rng(seed)
     idx = np.sort(rng.choice(batch.nsys, size=min(sample, batch.nsys), replace=False))
     sub = subset(batch, idx)
     if batch.kind == "solve":
-        xr, sr = oracle.solve(sub, "port", threads=oracle.host_threads())
+        xr, sr = oracle.solve(sub, which, threads=oracle.host_threads())
         worst, codes = 0.0, True
         for j, s in enumerate(idx):
             codes &= int(status_np[s]) == int(sr[j])
@@ -356,7 +379,7 @@ def accuracy(batch, out_np, status_np, mode, sample=512, seed=1):
             if sig.any():
                 worst = max(worst, float(np.max(np.abs(v[sig] - r[sig]) / np.abs(r[sig]))))
         return worst, bool(codes), "populations above 1e-20 of each system's total, max relative error"
-    ir, sr = oracle.invert(sub, "port", threads=oracle.host_threads())
+    ir, sr = oracle.invert(sub, which, threads=oracle.host_threads())
     worst, codes = 0.0, True
     for j, s in enumerate(idx):
         codes &= int(status_np[s]) == int(sr[j])
@@ -384,12 +407,13 @@ def run_ours(args):
     modes = []
     for b in batches:
         if args.mode == "auto":
-            # the fastest path that meets the 1e-10 bar against the reference on
-            # every system is the GSL-exact FP64 one (see the accuracy study)
-            modes.append("fp64")
+            # ion-balance solves: only the GSL-exact FP64 path meets the 1e-10 bar
+            # against the reference (its own answers are that far from exact);
+            # macro-atom inverses: the certified path
+            modes.append("fp64" if b.kind == "solve" else "fast")
         else:
             modes.append(args.mode)
-    code = {"fp64": engine.FP64, "mixed": engine.MIXED}
+    code = {"fp64": engine.FP64, "mixed": engine.MIXED, "fast": engine.FAST}
     plans, bufs = [], []
     for b, m in zip(batches, modes):
         plans.append(engine.Plan(b, code[m]))
@@ -480,12 +504,12 @@ def run_ours(args):
         err, codes_ok, what = accuracy(b, out.cpu().numpy(), st.cpu().numpy(), m)
         d = diag.cpu().numpy()
         acc.append({"kind": b.kind, "mode": m, "max_rel_err": err, "codes_match": codes_ok, "measure": what,
-                    "fallback_frac": float(np.mean((d & (1 << 8)) != 0)) if m == "mixed" else 0.0})
+                    "exact_path_frac": float(np.mean((d & (1 << 8)) != 0))})
 
     # ---- dominant kernel: the size class with the most flops, timed alone --
     best = None
     for b, m in zip(batches, modes):
-        classes = np.array([size_class(int(n)) for n in b.n])
+        classes = np.array([size_class(int(n), b.kind, m) for n in b.n])
         for c in np.unique(classes):
             idx = np.nonzero(classes == c)[0]
             nn = b.n[idx].astype(np.float64)
@@ -519,20 +543,27 @@ def run_ours(args):
     hbm_peak, peak_src = measured_peaks()
     fp64_peak = fp64_peak_tflops(device)
     traffic, traffic_src = args.traffic, "--traffic"
-    if traffic is None and args.config in TRAFFIC and TRAFFIC[args.config][0] == dc and args.nsys is None:
-        traffic = TRAFFIC[args.config][1] * alg_bytes
-        traffic_src = TRAFFIC[args.config][2]
-    roofline = {"bound": "hbm", "achieved": alg_bytes / t_kernel / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                "frac": alg_bytes / t_kernel / 1e9 / hbm_peak, "traffic": traffic,
-                "traffic_source": traffic_src if traffic is not None else None,
-                "kernel": kernel_name(dom.kind, dc, dm), "size_class": dc, "launch_s": t_kernel,
-                "bytes_per_launch": alg_bytes, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
-    t_roof = max(alg_bytes / (hbm_peak * 1e9), alg_flops / (fp64_peak * 1e12))
-    roofline_fp64 = {"bound": "fp64", "achieved": alg_flops / t_kernel / 1e12, "peak": fp64_peak,
-                     "unit": "TFLOP/s", "frac": alg_flops / t_kernel / 1e12 / fp64_peak,
-                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul",
-                     "roofline_time_s": t_roof, "roofline_time_frac": t_roof / t_kernel,
-                     "flops_per_launch": alg_flops}
+    if traffic is None:
+        ratio, src = traffic_ratio(dc)
+        if ratio is not None:
+            traffic = ratio * alg_bytes
+            traffic_src = f"{src}: DRAM bytes / algorithmic bytes of that capture ({ratio:.3f}) x this launch's bytes"
+    # the roofline of the launch is the slower of matrix bytes at HBM bandwidth
+    # and algorithmic flops at the FP64 peak; `roofline` reports the binding one
+    t_hbm = alg_bytes / (hbm_peak * 1e9)
+    t_fp64 = alg_flops / (fp64_peak * 1e12)
+    hbm_line = {"bound": "hbm", "achieved": alg_bytes / t_kernel / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": t_hbm / t_kernel, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
+    fp64_line = {"bound": "fp64", "achieved": alg_flops / t_kernel / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                 "frac": t_fp64 / t_kernel,
+                 "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (MEASURED_PEAKS.json "
+                                "has no FP64 entry)"}
+    roofline = dict(fp64_line if t_fp64 >= t_hbm else hbm_line)
+    roofline.update({"traffic": traffic, "traffic_source": traffic_src if traffic is not None else None,
+                     "kernel": kernel_name(dom.kind, dc, dm), "size_class": dc, "launch_s": t_kernel,
+                     "bytes_per_launch": alg_bytes, "flops_per_launch": alg_flops,
+                     "systems_per_launch": dom.nsys})
+    roofline_other = fp64_line if t_fp64 < t_hbm else hbm_line
     dplan.close()
     del flush
 
@@ -616,9 +647,9 @@ def run_ours(args):
             cus = {"value": nsys_step / t_sys, "unit": UNIT, "sample": " + ".join(i["sample"] for i in infos),
                    "max_rel_err_vs_gsl": max(i["max_rel_err_vs_gsl"] for i in infos)}
 
-    # plain FP64 batched kernel on the same workload, for the mixed-vs-FP64 ratio
+    # plain FP64 batched kernels (every system GSL-exact) on the same workload
     fp64_value = None
-    if any(m == "mixed" for m in modes):
+    if any(m != "fp64" for m in modes):
         fplans = [engine.Plan(b, engine.FP64) for b in batches]
         for _ in range(2):
             for p, (A, bb, out, st, diag) in zip(fplans, bufs):
@@ -637,19 +668,25 @@ def run_ours(args):
             p.close()
 
     if rank == 0:
+        mode_names = {"fp64": "GSL-exact FP64 (SIROCCO_FP64)", "fast": "certified FP64 (SIROCCO_FAST)",
+                      "mixed": "mixed FP32/FP64 (SIROCCO_MIXED)"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if all(m == "fp64" for m in modes) else "f32+f64",
+                "dtype": "f32+f64" if any(m == "mixed" for m in modes) else "f64",
                 "data": "synthetic (seeded generators with the reference's structure)",
-                "config": {"workload": WORKLOADS[args.config], "config_index": args.config,
-                           "systems_per_step": nsys_step, "modes": modes,
-                           "l2": (f"inputs {in_bytes / 2**20:.0f} MiB > 126 MiB L2" if in_bytes > L2_BYTES
-                                  else f"inputs {in_bytes / 2**20:.0f} MiB < L2: not flushed between steps"),
-                           "parallelism": f"replicas x{world}"},
+                "config": {"workload": WORKLOADS[args.config], "config_index": args.config},
+                "run": {"systems_per_step": nsys_step,
+                        "modes": {b.kind: mode_names[m] for b, m in zip(batches, modes)},
+                        "l2": (f"inputs {in_bytes / 2**20:.0f} MiB > 126 MiB L2: no flush needed"
+                               if in_bytes > L2_BYTES else
+                               f"inputs {in_bytes / 2**20:.0f} MiB < L2: not flushed between steps"),
+                        "parallelism": f"replicas x{world}"},
                 "accuracy": acc, "plain_fp64_value": fp64_value,
                 "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
-                "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
+                "mixed_over_fp64_note": ("value / plain_fp64_value: the timed modes against every system on the "
+                                         "GSL-exact FP64 path"),
+                "roofline": roofline, "roofline_other_bound": roofline_other, "cpu_baseline": cpu, "e2e": e2e,
                 "cusolver_reference": cus, "launch_modes": launch_modes, "gpu_launches": launches,
                 "clocks": clock_info}
         print(json.dumps(line), flush=True)
@@ -895,8 +932,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, default=1, choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", choices=["auto", "fp64", "mixed"], default="auto")
+    ap.add_argument("--config", type=int, default=3, choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", choices=["auto", "fp64", "mixed", "fast"], default="auto")
     ap.add_argument("--nsys", type=int, default=None,
                     help="systems (cells for config 3) instead of the workload's own count (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
