@@ -41,8 +41,9 @@
 // local rows tr + RT i and columns tc + CT j.  Each CTA also runs one pivot
 // warp that holds no tile.  Every block step moves only the two panels
 // through shared memory:
-//   S1  the holders of K's rows write R (transposed, RowPT[c][q]) into the
-//       shared memory of every CTA of the cluster; the holders of K's columns
+//   S1  the holders of K's rows write R (transposed, RowPT[c][q]); in a
+//       cluster the owner CTA's tile threads then copy that panel into every
+//       other CTA, 16 bytes per store; the holders of K's columns
 //       write C' (ColP[r][q], minus I on D's diagonal) locally; the holders of
 //       the next pivot block write its current values (Dnext);  cluster barrier
 //   S3  the tile threads form R' (RowNT[c][q]) from D^-1;     barrier
@@ -113,7 +114,8 @@ struct CgjShape {
   static_assert(P % (8 * CL) == 0 && LP % RT == 0 && P % CT == 0, "whole tiles");
   static_assert(NT % 32 == 0 && NTH <= 1024, "whole warps");
   static_assert(CT * LP <= 2 * buf, "certificate partials fit the panel buffers");
-  static_assert(CL == 1 || CL == 2 || CL == 4 || CL == 8, "portable cluster sizes");
+  static_assert((SP * P) % 2 == 0 && off_RowPT % 2 == 0, "16-byte copies of the row panel");
+  static_assert(CL >= 1 && CL <= 8, "portable cluster sizes");
   static_assert(off_stage % 2 == 0 && SLOT % 2 == 0, "16-byte aligned staging slots");
   static_assert(LP / 8 <= 32, "one lane of the pivot warp issues each block's copy");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
@@ -242,16 +244,6 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
         }
 #pragma unroll
       for (int j = 0; j < TC; ++j) RowPT[(tc + CT * j) * SP + q] = rowv[j];
-      if (CL > 1) {
-        cg::cluster_group cl = cg::this_cluster();
-#pragma unroll
-        for (int pr = 0; pr < CL; ++pr) {
-          if (pr == rank) continue;
-          double* rp = cl.map_shared_rank(RowPT, pr);
-#pragma unroll
-          for (int j = 0; j < TC; ++j) rp[(tc + CT * j) * SP + q] = rowv[j];
-        }
-      }
     }
     if ((tc >> 3) == kblk % CB) {
       const int jK = kblk / CB, q = tc & 7;
@@ -278,6 +270,25 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
           for (int j = 0; j < TC; ++j)
             if (i == iK1 && j == jK1) v = W[i][j];
         B[S::off_Dnext + (tr & 7) * SP + (tc & 7)] = v;
+      }
+    }
+  };
+
+  // cluster: the owner of block kblk copies its row panel into every other
+  // CTA once its tile threads have written it (a barrier over the tile threads
+  // only, so the pivot warp's work is not waited for), 16 bytes per store,
+  // consecutive threads on consecutive addresses
+  auto share_row_panel = [&](int kblk) {
+    if (CL > 1) {
+      asm volatile("bar.sync 1, %0;\n" ::"r"(NT) : "memory");
+      if (rank == kblk % CL) {
+        cg::cluster_group cl = cg::this_cluster();
+        const double2* src = reinterpret_cast<const double2*>(bufp(kblk) + S::off_RowPT);
+        for (int pr = 0; pr < CL; ++pr) {
+          if (pr == rank) continue;
+          double2* dst = reinterpret_cast<double2*>(cl.map_shared_rank(bufp(kblk) + S::off_RowPT, pr));
+          for (int e = tid; e < P * SP / 2; e += NT) dst[e] = src[e];
+        }
       }
     }
   };
@@ -450,7 +461,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     }
 
     // ---- prologue: the first pivot block and its inverse
-    if (tile) publish(0);
+    if (tile) {
+      publish(0);
+      share_row_panel(0);
+    }
     cluster_barrier<CL>();
     if (!tile && rank == 0) {
       const double* RowPT = bufp(0) + S::off_RowPT;
@@ -469,7 +483,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
       const int kb = 8 * kblk;
 
       if (kblk > 0) {
-        if (tile) publish(kblk);
+        if (tile) {
+          publish(kblk);
+          share_row_panel(kblk);
+        }
         cluster_barrier<CL>();   // also orders the pivot warp's D^-1 of this block
       }
 
