@@ -414,6 +414,8 @@ def run_ours(args):
         else:
             modes.append(args.mode)
     code = {"fp64": engine.FP64, "mixed": engine.MIXED, "fast": engine.FAST}
+    if args.only_dominant:
+        return run_dominant(args, engine, batches, modes, code, device)
     plans, bufs = [], []
     for b, m in zip(batches, modes):
         plans.append(engine.Plan(b, code[m]))
@@ -507,16 +509,7 @@ def run_ours(args):
                     "exact_path_frac": float(np.mean((d & (1 << 8)) != 0))})
 
     # ---- dominant kernel: the size class with the most flops, timed alone --
-    best = None
-    for b, m in zip(batches, modes):
-        classes = np.array([size_class(int(n), b.kind, m) for n in b.n])
-        for c in np.unique(classes):
-            idx = np.nonzero(classes == c)[0]
-            nn = b.n[idx].astype(np.float64)
-            fl = float(np.sum(2.0 / 3.0 * nn ** 3 + 2 * nn ** 2 if b.kind == "solve" else 2.0 * nn ** 3))
-            if best is None or fl > best[0]:
-                best = (fl, b, m, c, idx)
-    fl, db, dm, dc, didx = best
+    fl, db, dm, dc, didx = dominant_class(batches, modes)
     dom = db if didx.size == db.nsys else subset(db, didx)
     dplan = engine.Plan(dom, code[dm])
     dA = torch.from_numpy(dom.A).to(device)
@@ -694,6 +687,48 @@ def run_ours(args):
         p.close()
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def dominant_class(batches, modes):
+    """The size class with the most algorithmic flops: (flops, batch, mode, class, indices)."""
+    best = None
+    for b, m in zip(batches, modes):
+        classes = np.array([size_class(int(n), b.kind, m) for n in b.n])
+        for c in np.unique(classes):
+            idx = np.nonzero(classes == c)[0]
+            nn = b.n[idx].astype(np.float64)
+            fl = float(np.sum(2.0 / 3.0 * nn ** 3 + 2 * nn ** 2 if b.kind == "solve" else 2.0 * nn ** 3))
+            if best is None or fl > best[0]:
+                best = (fl, b, m, c, idx)
+    return best
+
+
+def run_dominant(args, engine, batches, modes, code, device):
+    """Profiling case (--only-dominant): the workload's dominant size class alone,
+    W + K launches of its plan and nothing else, so that an ncu capture of that
+    kernel can select launches by count."""
+    import torch
+    fl, db, dm, dc, didx = dominant_class(batches, modes)
+    dom = db if didx.size == db.nsys else subset(db, didx)
+    plan = engine.Plan(dom, code[dm])
+    A = torch.from_numpy(dom.A).to(device)
+    out = torch.empty(dom.b.size if dom.kind == "solve" else dom.A.size, dtype=torch.float64, device=device)
+    st = torch.empty((dom.nsys,), dtype=torch.int32, device=device)
+    bb = torch.from_numpy(dom.b).to(device) if dom.kind == "solve" else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        plan.execute(A, out, st, b=bb)
+    e0.record()
+    for _ in range(args.steps):
+        plan.execute(A, out, st, b=bb)
+    e1.record()
+    torch.cuda.synchronize(device)
+    t = e0.elapsed_time(e1) / 1e3 / max(1, args.steps)
+    print(json.dumps({"profiling_case": kernel_name(dom.kind, dc, dm), "size_class": dc, "systems": dom.nsys,
+                      "bytes": dom.bytes(), "flops": dom.flops(), "launch_s": t,
+                      "launches_per_execute": plan.launches}), flush=True)
+    plan.close()
     return 0
 
 
@@ -937,6 +972,8 @@ def main(argv=None):
     ap.add_argument("--nsys", type=int, default=None,
                     help="systems (cells for config 3) instead of the workload's own count (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only-dominant", action="store_true",
+                    help="profiling case: launch only the dominant size class's plan (W + K times)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cusolver", action="store_true",
