@@ -35,34 +35,43 @@
 // entry takes the same fused update and no thread branches on where it sits.
 //
 // Layout: the padded P x P matrix is RESIDENT IN REGISTERS for the whole
-// factorisation, spread over the tile threads of one CTA or of a cluster of CL
+// factorisation, spread over the tile warps of one CTA or of a cluster of CL
 // CTAs (one SM each).  Rows go to the cluster's CTAs in blocks of 8 (block b to
-// CTA b % CL); inside a CTA, tile thread (tr, tc) of an RT x CT grid holds
-// local rows tr + RT i and columns tc + CT j.  Each CTA also runs one pivot
-// warp that holds no tile.  Every block step moves only the two panels
-// through shared memory:
-//   S1  the holders of K's rows write R (transposed, RowPT[c][q]); in a
+// CTA b % CL).  A CTA's rows and all columns form 8 x 8 sub-blocks; tile warp
+// (wr, wc) of a WGR x WGC warp grid owns local row blocks wr + WGR i and column
+// blocks wc + WGC j, each sub-block held as the accumulator fragment of the
+// FP64 tensor-core MMA (mma.sync m8n8k4 f64: lane l holds row l/4, columns
+// 2(l%4) and 2(l%4)+1).  Each CTA also runs one pivot warp that holds no tile.
+// Every block step moves only the two panels through shared memory:
+//   S1  the warps holding K's rows write R (transposed, RowPT[c][q]); in a
 //       cluster the owner CTA's tile threads then copy that panel into every
-//       other CTA, 16 bytes per store; the holders of K's columns
-//       write C' (ColP[r][q], minus I on D's diagonal) locally; the holders of
-//       the next pivot block write its current values (Dnext);  cluster barrier
-//   S3  the tile threads form R' (RowNT[c][q]) from D^-1;     barrier
-//   S4  every tile thread updates its tile, W -= C' R', while the pivot warp of
-//       the CTA that owns the next block brings Dnext up to date with the same
-//       fused multiply-adds, in the same order, and inverts it (8 x 8, two
-//       entries per lane, shuffles), writing D^-1 of the next step into every
-//       CTA of the cluster.
+//       other CTA, 16 bytes per store; the warps holding K's columns write
+//       -C' (ColPN[r][q] = I - C on D's diagonal, -C elsewhere) locally; the
+//       holder of the next pivot block writes its current values (Dnext);
+//                                                               cluster barrier
+//   S3  the tile warps form R' = D^-1 R (RowNT[c][q]), two MMAs per 8-column
+//       block;                                                  barrier
+//   S4  every tile warp adds (-C') R' into each of its sub-blocks, two MMAs per
+//       sub-block from one operand load per row and per column block, while
+//       the pivot warp of the CTA that owns the next block brings Dnext up to
+//       date with the same MMAs in the same order and inverts it (8 x 8, the
+//       accumulator fragment's two entries per lane, shuffles), writing D^-1 of
+//       the next step into every CTA of the cluster.
 // So the serial 8 x 8 inverse overlaps the bulk update, and a step costs two
-// barriers.
+// barriers.  Panel rows hold 8 values at a stride of SP = 12 doubles: the
+// operand fragments (8 panel rows x 4 values per load) then fall on distinct
+// banks.  The row panel, -C', D^-1 and Dnext are double-buffered by step
+// parity; R' needs one buffer.  B200's FP64 tensor-core MMA runs
+// at the FP64 FMA rate (both ~37 TF/s here); it is used for its eight-fold
+// fewer issued instructions and its operand reuse across a warp, and it keeps
+// the FMA pipe free for the pivot warp's chain.
 // Staging: the rows a CTA holds arrive in shared memory by 1-D TMA bulk copies
 // (cp.async.bulk, one per 8-row block, completing on an mbarrier), issued for
 // the NEXT matrix as soon as the current one has moved into registers, so the
 // HBM latency of a matrix overlaps the factorisation of the one before.  A bulk
 // copy needs 16-byte aligned ends: the aligned interior of each block is
 // copied, and the at most two 8-byte ends are read by plain loads, so nothing
-// outside the caller's matrix is touched.  Panel rows are 8 values at an odd stride of SP = 9 doubles, so the
-// 8-byte loads of S3 and S4 -- at most 32 distinct panel rows per warp, the
-// rest broadcasts -- hit distinct banks; panel buffers are double-buffered.
+// outside the caller's matrix is touched.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -81,43 +90,44 @@ struct CertArgs {
   int* fb_count;       // [classes] entries appended (zeroed before the launch)
 };
 
-// P: padded order; RT x CT: tile-thread grid of one CTA; CL: CTAs per matrix
-// (a cluster); MINB: CTAs per SM asked of the register allocator.
-template <int P_, int RT_, int CT_, int CL_, int MINB_>
+// P: padded order; WGR x WGC: tile-warp grid of one CTA; CL: CTAs per matrix (a
+// cluster); MINB: CTAs per SM asked of the register allocator.
+template <int P_, int WGR_, int WGC_, int CL_, int MINB_>
 struct CgjShape {
-  static constexpr int P = P_, RT = RT_, CT = CT_, CL = CL_;
-  static constexpr int NT = RT * CT;       // tile threads
+  static constexpr int P = P_, WGR = WGR_, WGC = WGC_, CL = CL_;
+  static constexpr int NW = WGR * WGC;     // tile warps
+  static constexpr int NT = 32 * NW;       // tile threads
   static constexpr int NTH = NT + 32;      // with the pivot warp
   static constexpr int LP = P / CL;        // rows held by one CTA
-  static constexpr int TR = LP / RT;       // rows per tile thread
-  static constexpr int TC = P / CT;        // columns per tile thread
-  static constexpr int RB = RT / 8;        // 8-row blocks spanned by the thread rows
-  static constexpr int CB = CT / 8;
+  static constexpr int LB = LP / 8;        // local 8-row blocks
+  static constexpr int CBK = P / 8;        // 8-column blocks
+  static constexpr int WR = LB / WGR;      // row blocks per tile warp
+  static constexpr int WC = CBK / WGC;     // column blocks per tile warp
   static constexpr int MINB = MINB_;
-  static constexpr int SP = 9;             // stride of a panel row (8 values)
-  // shared memory, in doubles, per panel buffer
+  static constexpr int SP = 12;            // stride of a panel row (8 values)
+  // shared memory, in doubles, per panel buffer (two buffers, by step parity)
   static constexpr int off_RowPT = 0;                   // [P][SP]
-  static constexpr int off_RowNT = SP * P;              // [P][SP]
-  static constexpr int off_ColP = 2 * SP * P;           // [LP][SP]
-  static constexpr int off_Dinv = 2 * SP * P + SP * LP; // [8][SP]
+  static constexpr int off_ColP = SP * P;               // [LP][SP]  -C'
+  static constexpr int off_Dinv = SP * P + SP * LP;     // [8][SP]
   static constexpr int off_Dnext = off_Dinv + 8 * SP;   // [8][SP]
   static constexpr int buf = off_Dnext + 8 * SP;
-  static constexpr int off_dg = 2 * buf;                // [LP] diagonal of each local row
+  // R' has one buffer: S3 writes it after a step's first barrier and the last
+  // reader (S4 and the pivot warp) is done before the next step's first barrier
+  static constexpr int off_RowNT = 2 * buf;             // [P][SP]
+  static constexpr int off_dg = off_RowNT + SP * P;     // [LP] diagonal of each local row
   static constexpr int off_ok = off_dg + LP;            // [2][8] certificate of each CTA, by item parity
   static constexpr int off_bar = off_ok + 16;           // the staging mbarrier (8 bytes)
   static constexpr int SLOT = 8 * P + 2;                // doubles per staged 8-row block (+ alignment shift)
-  static constexpr int off_stage = off_bar + 2;         // [LP / 8][SLOT], 16-byte aligned
-  static constexpr int n_dbl = off_stage + (LP / 8) * SLOT;
+  static constexpr int off_stage = off_bar + 2;         // [LB][SLOT], 16-byte aligned
+  static constexpr int n_dbl = off_stage + LB * SLOT;
   static constexpr size_t dyn_smem = size_t(n_dbl) * 8;
-  static_assert(RT % 8 == 0 && CT % 8 == 0, "8-row / 8-column pivot blocks map onto whole thread groups");
-  static_assert(CT <= 32, "a thread row's partial sums fit the reduction buffer");
-  static_assert(P % (8 * CL) == 0 && LP % RT == 0 && P % CT == 0, "whole tiles");
-  static_assert(NT % 32 == 0 && NTH <= 1024, "whole warps");
-  static_assert(CT * LP <= 2 * buf, "certificate partials fit the panel buffers");
-  static_assert((SP * P) % 2 == 0 && off_RowPT % 2 == 0, "16-byte copies of the row panel");
+  static_assert(P % (8 * CL) == 0 && LB % WGR == 0 && CBK % WGC == 0, "whole sub-block tiles");
+  static_assert(NTH <= 1024, "one CTA");
+  static_assert(WGC * LP <= 2 * buf, "certificate partials fit the panel buffers");
   static_assert(CL >= 1 && CL <= 8, "portable cluster sizes");
   static_assert(off_stage % 2 == 0 && SLOT % 2 == 0, "16-byte aligned staging slots");
-  static_assert(LP / 8 <= 32, "one lane of the pivot warp issues each block's copy");
+  static_assert((SP * P) % 2 == 0 && buf % 2 == 0 && off_dg % 2 == 0, "16-byte copies of the row panel");
+  static_assert(LB <= 32, "one lane of the pivot warp issues each block's copy");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
 };
 
@@ -171,10 +181,20 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // polls of a staging wait: about a second, far beyond any copy's duration
 constexpr int kStageWaitPolls = 1 << 24;
 
+// d[0..1] += A (8 x 4, lane l: row l/4, column l%4) * B (4 x 8, lane l: row
+// l%4, column l/4), FP64 on the tensor cores; d is the accumulator fragment
+// (lane l: row l/4, columns 2(l%4) and 2(l%4)+1).
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 // In-place Gauss-Jordan inverse of the 8 x 8 pivot block by one warp, without
-// pivoting.  Lane l holds D[l/4][2(l%4)] in d0 and D[l/4][2(l%4)+1] in d1.
-// (Measured alone on an SM: ~910 cycles per call; a variant taking two pivots
-// at a time through 2 x 2 determinants needed more shuffles and took ~1250.)
+// pivoting.  Lane l holds D[l/4][2(l%4)] in d0 and D[l/4][2(l%4)+1] in d1 (the
+// accumulator fragment's layout).  (Measured alone on an SM: ~910 cycles per
+// call; a variant taking two pivots at a time through 2 x 2 determinants
+// needed more shuffles and took ~1250.)
 __device__ __forceinline__ void warp_inv8(double& d0, double& d1, int lane) {
   const int q = lane >> 2, h = lane & 3;
 #pragma unroll
@@ -198,78 +218,85 @@ __device__ __forceinline__ void warp_inv8(double& d0, double& d1, int lane) {
   }
 }
 
-template <int P, int RT, int CT, int CL, int MINB>
-__global__ void __launch_bounds__(RT* CT + 32, MINB)
+template <int P, int WGR, int WGC, int CL, int MINB>
+__global__ void __launch_bounds__(32 * WGR * WGC + 32, MINB)
 cgj_inverse_kernel(BatchView bv, CertArgs ca) {
-  using S = CgjShape<P, RT, CT, CL, MINB>;
-  constexpr int NT = S::NT, TR = S::TR, TC = S::TC, LP = S::LP, RB = S::RB, CB = S::CB, SP = S::SP;
-  constexpr int NBLK = P / 8;
+  using S = CgjShape<P, WGR, WGC, CL, MINB>;
+  constexpr int NW = S::NW, NT = S::NT, WR = S::WR, WC = S::WC, LP = S::LP, LB = S::LB, CBK = S::CBK;
+  constexpr int SP = S::SP, NBLK = P / 8;
   extern __shared__ __align__(16) double sm[];
   namespace cg = cooperative_groups;
 
   const int tid = threadIdx.x;
-  const bool tile = tid < NT;                 // warp-uniform: NT is a multiple of 32
-  const int tr = tid / CT, tc = tid % CT;     // meaningful for tile threads
-  const int lane = tid & 31;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;      // fragment row, column pair
+  const bool tile = warp < NW;                // the last warp is the pivot warp
+  const int wr = warp / WGC, wc = warp % WGC;  // meaningful for tile warps
   const int rank = (CL > 1) ? int(cluster_rank()) : 0;
   const int cid = blockIdx.x / CL, ncl = gridDim.x / CL;
   const int cnt = batch_count(bv);
 
-  // global row of this thread's local row i (blocks of 8 rows dealt to the CTAs)
-  auto grow = [&](int i) -> int {
-    const int lr = tr + RT * i;
-    return (((lr >> 3) * CL) + rank) * 8 + (lr & 7);
-  };
+  // local row (in this CTA) and global row of this lane's row in sub-block row i,
+  // global column of its column e in sub-block column j
+  auto lrow = [&](int i) -> int { return (wr + WGR * i) * 8 + g; };
+  auto grow = [&](int i) -> int { return ((wr + WGR * i) * CL + rank) * 8 + g; };
+  auto gcol = [&](int j, int e) -> int { return (wc + WGC * j) * 8 + 2 * t + e; };
   auto bufp = [&](int kblk) -> double* { return sm + (kblk & 1) * S::buf; };
-  double W[TR][TC];
+  double W[WR][WC][2];
 
-  // S1 of block kblk: the old row panel (to every CTA), the old column panel
-  // minus I on D's diagonal, and the current values of the next pivot block
+  // S1 of block kblk: the old row panel, -C' and the next pivot block's values
   auto publish = [&](int kblk) {
     double* B = bufp(kblk);
     double* RowPT = B + S::off_RowPT;
     double* ColP = B + S::off_ColP;
     const int kb = 8 * kblk;
-    const int owner = kblk % CL, lbK = kblk / CL;
-    if (rank == owner && (tr >> 3) == lbK % RB) {
-      const int iK = lbK / RB, q = tr & 7;
-      double rowv[TC];
+    const int lbK = kblk / CL;
+    if (rank == kblk % CL && wr == lbK % WGR) {
+      const int iK = lbK / WGR;
 #pragma unroll
-      for (int j = 0; j < TC; ++j) rowv[j] = W[0][j];
+      for (int j = 0; j < WC; ++j) {
+        double v0 = W[0][j][0], v1 = W[0][j][1];
 #pragma unroll
-      for (int i = 1; i < TR; ++i)
-        if (i == iK) {
-#pragma unroll
-          for (int j = 0; j < TC; ++j) rowv[j] = W[i][j];
-        }
-#pragma unroll
-      for (int j = 0; j < TC; ++j) RowPT[(tc + CT * j) * SP + q] = rowv[j];
+        for (int i = 1; i < WR; ++i)
+          if (i == iK) {
+            v0 = W[i][j][0];
+            v1 = W[i][j][1];
+          }
+        RowPT[gcol(j, 0) * SP + g] = v0;
+        RowPT[gcol(j, 1) * SP + g] = v1;
+      }
     }
-    if ((tc >> 3) == kblk % CB) {
-      const int jK = kblk / CB, q = tc & 7;
-      double colv[TR];
+    if (wc == kblk % WGC) {
+      const int jK = kblk / WGC;
 #pragma unroll
-      for (int i = 0; i < TR; ++i) colv[i] = W[i][0];
+      for (int i = 0; i < WR; ++i) {
+        double v0 = W[i][0][0], v1 = W[i][0][1];
 #pragma unroll
-      for (int j = 1; j < TC; ++j)
-        if (j == jK) {
-#pragma unroll
-          for (int i = 0; i < TR; ++i) colv[i] = W[i][j];
-        }
-#pragma unroll
-      for (int i = 0; i < TR; ++i) ColP[(tr + RT * i) * SP + q] = colv[i] - ((grow(i) == kb + q) ? 1.0 : 0.0);
+        for (int j = 1; j < WC; ++j)
+          if (j == jK) {
+            v0 = W[i][j][0];
+            v1 = W[i][j][1];
+          }
+        const int r = grow(i);
+        ColP[lrow(i) * SP + 2 * t] = ((r == kb + 2 * t) ? 1.0 : 0.0) - v0;
+        ColP[lrow(i) * SP + 2 * t + 1] = ((r == kb + 2 * t + 1) ? 1.0 : 0.0) - v1;
+      }
     }
     if (kblk + 1 < NBLK) {
       const int k1 = kblk + 1, lbK1 = k1 / CL;
-      if (rank == k1 % CL && (tr >> 3) == lbK1 % RB && (tc >> 3) == k1 % CB) {
-        const int iK1 = lbK1 / RB, jK1 = k1 / CB;
-        double v = W[0][0];
+      if (rank == k1 % CL && wr == lbK1 % WGR && wc == k1 % WGC) {
+        const int i1 = lbK1 / WGR, j1 = k1 / WGC;
+        double v0 = W[0][0][0], v1 = W[0][0][1];
 #pragma unroll
-        for (int i = 0; i < TR; ++i)
+        for (int i = 0; i < WR; ++i)
 #pragma unroll
-          for (int j = 0; j < TC; ++j)
-            if (i == iK1 && j == jK1) v = W[i][j];
-        B[S::off_Dnext + (tr & 7) * SP + (tc & 7)] = v;
+          for (int j = 0; j < WC; ++j)
+            if (i == i1 && j == j1) {
+              v0 = W[i][j][0];
+              v1 = W[i][j][1];
+            }
+        B[S::off_Dnext + g * SP + 2 * t] = v0;
+        B[S::off_Dnext + g * SP + 2 * t + 1] = v1;
       }
     }
   };
@@ -293,22 +320,21 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     }
   };
 
-  // the pivot warp: D^-1 of block kblk from the 8 x 8 values d0, d1 (lane
-  // layout of warp_inv8), written into every CTA's buffer of that block
+  // the pivot warp: D^-1 of block kblk from the 8 x 8 values d0, d1
+  // (accumulator layout), written into every CTA's buffer of that block
   auto pivot_inverse = [&](int kblk, double d0, double d1) {
     warp_inv8(d0, d1, lane);
     double* Dinv = bufp(kblk) + S::off_Dinv;
-    const int q = lane >> 2, h = lane & 3;
-    Dinv[q * SP + 2 * h] = d0;
-    Dinv[q * SP + 2 * h + 1] = d1;
+    Dinv[g * SP + 2 * t] = d0;
+    Dinv[g * SP + 2 * t + 1] = d1;
     if (CL > 1) {
       cg::cluster_group cl = cg::this_cluster();
 #pragma unroll
       for (int pr = 0; pr < CL; ++pr) {
         if (pr == rank) continue;
         double* rp = cl.map_shared_rank(Dinv, pr);
-        rp[q * SP + 2 * h] = d0;
-        rp[q * SP + 2 * h + 1] = d1;
+        rp[g * SP + 2 * t] = d0;
+        rp[g * SP + 2 * t + 1] = d1;
       }
     }
   };
@@ -331,8 +357,8 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
   auto stage_issue = [&](int it) {   // the pivot warp, all lanes
     const int s2 = bv.list[it];
     unsigned bytes = 0;
-    uintptr_t i0 = 0, b0, b1;
-    if (lane < LP / 8 && block_span(s2, lane, b0, b1)) {
+    uintptr_t i0 = 0, b0 = 0, b1 = 0;
+    if (lane < LB && block_span(s2, lane, b0, b1)) {
       i0 = (b0 + 15) & ~uintptr_t(15);
       const uintptr_t i1 = b1 & ~uintptr_t(15);
       if (i1 > i0) bytes = unsigned(i1 - i0);
@@ -350,13 +376,13 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
   // the ends of each block that the aligned copy leaves out, by plain loads
   auto stage_ends = [&](int s2) {    // the pivot warp
     uintptr_t b0, b1;
-    if (lane < LP / 8 && block_span(s2, lane, b0, b1)) {
+    if (lane < LB && block_span(s2, lane, b0, b1)) {
       const int shift = int((b0 >> 3) & 1);
       double* slot = stage + lane * S::SLOT + shift;
-      const double* g = reinterpret_cast<const double*>(b0);
+      const double* gp = reinterpret_cast<const double*>(b0);
       const int64_t ne = int64_t((b1 - b0) >> 3);
-      if (shift) slot[0] = g[0];                                   // head: b0 not 16-byte aligned
-      if ((b1 & 15) && (ne > 1 || !shift)) slot[ne - 1] = g[ne - 1];   // tail: b1 not 16-byte aligned
+      if (shift) slot[0] = gp[0];                                      // head: b0 not 16-byte aligned
+      if ((b1 & 15) && (ne > 1 || !shift)) slot[ne - 1] = gp[ne - 1];   // tail: b1 not 16-byte aligned
     }
   };
   if (!tile) {
@@ -381,42 +407,42 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     sphase ^= 1;
     if (!tile && !stalled) stage_ends(s);
     __syncthreads();
-    double* red = sm;   // [CT][LP] partial off-diagonal sums, over the panel buffers
+    double* red = sm;   // [WGC][LP] partial off-diagonal sums, over the panel buffers
     double* dg = sm + S::off_dg;
     bool zok = !stalled;
     if (tile) {
-      int shift[TR];
 #pragma unroll
-      for (int i = 0; i < TR; ++i) {
+      for (int i = 0; i < WR; ++i) {
         uintptr_t b0, b1;
-        const int lb = (tr + RT * i) >> 3;
-        shift[i] = block_span(s, lb, b0, b1) ? int((b0 >> 3) & 1) : 0;
-      }
-#pragma unroll
-      for (int i = 0; i < TR; ++i) {
+        const int lb = wr + WGR * i;
+        const int shift = block_span(s, lb, b0, b1) ? int((b0 >> 3) & 1) : 0;
+        const double* slot = stage + lb * S::SLOT + shift + g * n;
         const int r = grow(i);
-        const double* slot = stage + ((tr + RT * i) >> 3) * S::SLOT + shift[i] + ((tr + RT * i) & 7) * n;
         double part = 0.0;
 #pragma unroll
-        for (int j = 0; j < TC; ++j) {
-          const int c = tc + CT * j;
-          const double a = (r < n && c < n) ? slot[c] : ((r == c) ? 1.0 : 0.0);
-          W[i][j] = a;
-          if (c == r) {
-            dg[tr + RT * i] = a;
-          } else {
-            zok &= (a <= 0.0);    // false for NaN
-            part += fabs(a);
+        for (int j = 0; j < WC; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int c = gcol(j, e);
+            const double a = (r < n && c < n) ? slot[c] : ((r == c) ? 1.0 : 0.0);
+            W[i][j][e] = a;
+            if (c == r) {
+              dg[lrow(i)] = a;
+            } else {
+              zok &= (a <= 0.0);    // false for NaN
+              part += fabs(a);
+            }
           }
-        }
-        red[tc * LP + tr + RT * i] = part;
+        part += __shfl_xor_sync(0xffffffffu, part, 1);
+        part += __shfl_xor_sync(0xffffffffu, part, 2);
+        if (t == 0) red[wc * LP + lrow(i)] = part;
       }
     }
     __syncthreads();
     bool rok = true;
     for (int lr = tid; lr < LP; lr += S::NTH) {
       double off = 0.0;
-      for (int t = 0; t < CT; ++t) off += red[t * LP + lr];
+      for (int q = 0; q < WGC; ++q) off += red[q * LP + lr];
       const double d = dg[lr];
       rok &= (d > 0.0) && (d < INFINITY) && (off * (1.0 + 0x1p-40) <= (1.0 - kCertMargin) * d);
     }
@@ -468,8 +494,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     cluster_barrier<CL>();
     if (!tile && rank == 0) {
       const double* RowPT = bufp(0) + S::off_RowPT;
-      const int q = lane >> 2, h = lane & 3;
-      pivot_inverse(0, RowPT[(2 * h) * SP + q], RowPT[(2 * h + 1) * SP + q]);
+      pivot_inverse(0, RowPT[(2 * t) * SP + g], RowPT[(2 * t + 1) * SP + g]);
     }
     cluster_barrier<CL>();
 
@@ -477,7 +502,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     for (int kblk = 0; kblk < NBLK; ++kblk) {
       double* B = bufp(kblk);
       const double* RowPT = B + S::off_RowPT;
-      double* RowNT = B + S::off_RowNT;
+      double* RowNT = sm + S::off_RowNT;
       const double* ColP = B + S::off_ColP;
       const double* Dinv = B + S::off_Dinv;
       const int kb = 8 * kblk;
@@ -490,56 +515,51 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
         cluster_barrier<CL>();   // also orders the pivot warp's D^-1 of this block
       }
 
-      // S3: R' = D^-1 R outside K, I + D^-1 on K's columns; a thread always
-      // forms entries of the same panel row q, so it reads row q of D^-1 once
+      // S3: R' = D^-1 R outside K, I + D^-1 on K's columns; an 8-column block
+      // per warp at a time, two MMAs with D^-1 as the row operand
       if (tile) {
-        const int q = tid & 7;
-        double dv[8];
-#pragma unroll
-        for (int p = 0; p < 8; ++p) dv[p] = Dinv[q * SP + p];
-#pragma unroll
-        for (int e0 = 0; e0 < 8 * P; e0 += NT) {
-          const int e = e0 + tid;
-          if (8 * P % NT != 0 && e >= 8 * P) break;
-          const int c = e >> 3;
-          double val = 0.0;
-#pragma unroll
-          for (int p = 0; p < 8; ++p) val = fma(dv[p], RowPT[c * SP + p], val);
-          const int ck = c - kb;
-          const bool inK = unsigned(ck) < 8u;
-          const double kv = Dinv[q * SP + (inK ? ck : 0)] + ((q == ck) ? 1.0 : 0.0);
-          RowNT[c * SP + q] = inK ? kv : val;
+        const double a0 = Dinv[g * SP + t], a1 = Dinv[g * SP + 4 + t];
+        for (int cb = warp; cb < CBK; cb += NW) {
+          double d[2];
+          if (cb == kblk) {
+            d[0] = Dinv[g * SP + 2 * t] + ((g == 2 * t) ? 1.0 : 0.0);
+            d[1] = Dinv[g * SP + 2 * t + 1] + ((g == 2 * t + 1) ? 1.0 : 0.0);
+          } else {
+            const double b0 = RowPT[(cb * 8 + g) * SP + t], b1 = RowPT[(cb * 8 + g) * SP + 4 + t];
+            d[0] = 0.0;
+            d[1] = 0.0;
+            dmma_884(d, a0, b0);
+            dmma_884(d, a1, b1);
+          }
+          RowNT[(cb * 8 + 2 * t) * SP + g] = d[0];
+          RowNT[(cb * 8 + 2 * t + 1) * SP + g] = d[1];
         }
       }
       __syncthreads();
 
       if (tile) {
-        // S4: W -= C' R'
+        // S4: W += (-C') R', two MMAs per sub-block
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          double cp[TR], rn[TC];
+        for (int h = 0; h < 2; ++h) {
+          double a[WR], b[WC];
 #pragma unroll
-          for (int i = 0; i < TR; ++i) cp[i] = ColP[(tr + RT * i) * SP + q];
+          for (int i = 0; i < WR; ++i) a[i] = ColP[lrow(i) * SP + 4 * h + t];
 #pragma unroll
-          for (int j = 0; j < TC; ++j) rn[j] = RowNT[(tc + CT * j) * SP + q];
+          for (int j = 0; j < WC; ++j) b[j] = RowNT[((wc + WGC * j) * 8 + g) * SP + 4 * h + t];
 #pragma unroll
-          for (int i = 0; i < TR; ++i)
+          for (int i = 0; i < WR; ++i)
 #pragma unroll
-            for (int j = 0; j < TC; ++j) W[i][j] = fma(-cp[i], rn[j], W[i][j]);
+            for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a[i], b[j]);
         }
       } else if (kblk + 1 < NBLK && rank == (kblk + 1) % CL) {
         // the next pivot block, updated exactly as its holders update it, then inverted
-        const int q = lane >> 2, h = lane & 3;
-        const int lr = ((kblk + 1) / CL) * 8 + q;     // local row of the next block's row q
+        const int lr0 = ((kblk + 1) / CL) * 8;
         const double* Dn = B + S::off_Dnext;
-        double d0 = Dn[q * SP + 2 * h], d1 = Dn[q * SP + 2 * h + 1];
+        double d[2] = {Dn[g * SP + 2 * t], Dn[g * SP + 2 * t + 1]};
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const double cpk = ColP[lr * SP + k];
-          d0 = fma(-cpk, RowNT[(kb + 8 + 2 * h) * SP + k], d0);
-          d1 = fma(-cpk, RowNT[(kb + 9 + 2 * h) * SP + k], d1);
-        }
-        pivot_inverse(kblk + 1, d0, d1);
+        for (int h = 0; h < 2; ++h)
+          dmma_884(d, ColP[(lr0 + g) * SP + 4 * h + t], RowNT[(kb + 8 + g) * SP + 4 * h + t]);
+        pivot_inverse(kblk + 1, d[0], d[1]);
       }
     }
 
@@ -547,14 +567,16 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     if (tile) {
       double* __restrict__ Og = bv.out + bv.offA[s];
 #pragma unroll
-      for (int i = 0; i < TR; ++i) {
+      for (int i = 0; i < WR; ++i) {
         const int r = grow(i);
         if (r < n) {
 #pragma unroll
-          for (int j = 0; j < TC; ++j) {
-            const int c = tc + CT * j;
-            if (c < n) Og[int64_t(r) * n + c] = W[i][j];
-          }
+          for (int j = 0; j < WC; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int c = gcol(j, e);
+              if (c < n) Og[int64_t(r) * n + c] = W[i][j][e];
+            }
         }
       }
     }
