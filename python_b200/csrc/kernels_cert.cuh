@@ -126,7 +126,7 @@ struct CgjShape {
   static_assert(WGC * LP <= 2 * buf, "certificate partials fit the panel buffers");
   static_assert(CL >= 1 && CL <= 8, "portable cluster sizes");
   static_assert(off_stage % 2 == 0 && SLOT % 2 == 0, "16-byte aligned staging slots");
-  static_assert((SP * P) % 2 == 0 && buf % 2 == 0 && off_dg % 2 == 0, "16-byte copies of the row panel");
+  static_assert(SP % 2 == 0 && buf % 2 == 0 && off_dg % 2 == 0, "16-byte copies of the row panel");
   static_assert(LB <= 32, "one lane of the pivot warp issues each block's copy");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
 };
@@ -314,7 +314,11 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
         for (int pr = 0; pr < CL; ++pr) {
           if (pr == rank) continue;
           double2* dst = reinterpret_cast<double2*>(cl.map_shared_rank(bufp(kblk) + S::off_RowPT, pr));
-          for (int e = tid; e < P * SP / 2; e += NT) dst[e] = src[e];
+          // the 8 values of each panel row, four 16-byte pieces, not the padding
+          for (int e = tid; e < 4 * P; e += NT) {
+            const int idx = (e >> 2) * (SP / 2) + (e & 3);
+            dst[idx] = src[idx];
+          }
         }
       }
     }
@@ -354,6 +358,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     b1 = b0 + uintptr_t(rb) * uintptr_t(n2) * 8u;
     return true;
   };
+  // the ends of each block that the aligned copy leaves out: read with plain
+  // loads when the copy is issued, kept in the issuing lane's registers, and
+  // written into the slot once the copy has landed
+  double head_v = 0.0, tail_v = 0.0;
   auto stage_issue = [&](int it) {   // the pivot warp, all lanes
     const int s2 = bv.list[it];
     unsigned bytes = 0;
@@ -362,6 +370,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
       i0 = (b0 + 15) & ~uintptr_t(15);
       const uintptr_t i1 = b1 & ~uintptr_t(15);
       if (i1 > i0) bytes = unsigned(i1 - i0);
+      const double* gp = reinterpret_cast<const double*>(b0);
+      const int64_t ne = int64_t((b1 - b0) >> 3);
+      head_v = gp[0];
+      tail_v = gp[ne - 1];
     }
     unsigned tot = bytes;
 #pragma unroll
@@ -373,16 +385,14 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
       bulk_g2s(stage + lane * S::SLOT + 2 * shift, reinterpret_cast<const void*>(i0), bytes, bar);
     }
   };
-  // the ends of each block that the aligned copy leaves out, by plain loads
   auto stage_ends = [&](int s2) {    // the pivot warp
     uintptr_t b0, b1;
     if (lane < LB && block_span(s2, lane, b0, b1)) {
       const int shift = int((b0 >> 3) & 1);
       double* slot = stage + lane * S::SLOT + shift;
-      const double* gp = reinterpret_cast<const double*>(b0);
       const int64_t ne = int64_t((b1 - b0) >> 3);
-      if (shift) slot[0] = gp[0];                                      // head: b0 not 16-byte aligned
-      if ((b1 & 15) && (ne > 1 || !shift)) slot[ne - 1] = gp[ne - 1];   // tail: b1 not 16-byte aligned
+      if (shift) slot[0] = head_v;                                     // head: b0 not 16-byte aligned
+      if ((b1 & 15) && (ne > 1 || !shift)) slot[ne - 1] = tail_v;       // tail: b1 not 16-byte aligned
     }
   };
   if (!tile) {
@@ -407,6 +417,21 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
     sphase ^= 1;
     if (!tile && !stalled) stage_ends(s);
     __syncthreads();
+    // the pivot warp of the CTA holding block 0 inverts D(0) straight from the
+    // staging slots while the tile warps check the certificate (wasted, and
+    // harmless, if the matrix fails it)
+    if (!tile && rank == 0 && !stalled) {
+      uintptr_t b0, b1;
+      const int shift = block_span(s, 0, b0, b1) ? int((b0 >> 3) & 1) : 0;
+      const double* slot = stage + shift + g * n;
+      double d[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = 2 * t + e;
+        d[e] = (g < n && c < n) ? slot[c] : ((g == c) ? 1.0 : 0.0);
+      }
+      pivot_inverse(0, d[0], d[1]);
+    }
     double* red = sm;   // [WGC][LP] partial off-diagonal sums, over the panel buffers
     double* dg = sm + S::off_dg;
     bool zok = !stalled;
@@ -486,15 +511,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
       continue;
     }
 
-    // ---- prologue: the first pivot block and its inverse
+    // ---- prologue: the first panels (D(0)^-1 is already in place)
     if (tile) {
       publish(0);
       share_row_panel(0);
-    }
-    cluster_barrier<CL>();
-    if (!tile && rank == 0) {
-      const double* RowPT = bufp(0) + S::off_RowPT;
-      pivot_inverse(0, RowPT[(2 * t) * SP + g], RowPT[(2 * t + 1) * SP + g]);
     }
     cluster_barrier<CL>();
 
