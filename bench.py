@@ -886,7 +886,11 @@ def run_rows(args):
         rc = lib.matom_matrices_batched(nsys, dn.ctypes.data, b.offA.ctypes.data, offv.ctypes.data, vp(dA), vp(dR),
                                         vp(dB), vp(dC), vp(dst))
         assert rc == 0, engine.last_error()
+    engine.set_precision(engine.FP64)
     t_matom = clock(matom)
+    engine.set_precision(engine.FAST)
+    t_matom_fast = clock(matom)
+    engine.set_precision(engine.FP64)
     dX = torch.empty_like(dA)
     plan = engine.Plan(b, engine.FP64)
 
@@ -894,6 +898,9 @@ def run_rows(args):
         plan.execute(dA, dX, dst)
         torch.cuda.synchronize(dev)
     t_inv = clock(inv_only)
+    plan.close()
+    plan = engine.Plan(b, engine.FAST)
+    t_inv_fast = clock(inv_only)
     plan.close()
     nq = 1 << 20
     rng = np.random.default_rng(5)
@@ -909,6 +916,9 @@ def run_rows(args):
     t_draw = clock(draws)
     out["matom_epilogue"] = {"workload": "8192 x n=61 inverse + B = N^-1 diag(R) + row running totals",
                              "systems_per_s": nsys / t_matom, "ms": t_matom * 1e3, "inverse_alone_ms": t_inv * 1e3,
+                             "certified_fused_ms": t_matom_fast * 1e3,
+                             "certified_inverse_alone_ms": t_inv_fast * 1e3,
+                             "certified_fused_systems_per_s": nsys / t_matom_fast,
                              "draws_per_s": nq / t_draw, "draws": nq}
     del dA, dR, dB, dC, dX
     # ion rate matrices: a 181-ion table (13 elements, H to Ni), 20,000 cells

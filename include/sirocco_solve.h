@@ -275,7 +275,10 @@ int macro_pops_lockstep(int ncell, int n, int nion, const int *ion_first, const 
 /* Macro-atom jumping matrices of a whole cycle (the reference's
    calc_matom_matrix, source/macro_accelerate.c:311-334, called per cell from
    calc_all_matom_matrices :1054-1061).  For every cell s, N_s = I - Q/Q_norm
-   (n[s] x n[s], row-major at offA[s]) is inverted GSL-exactly and
+   (n[s] x n[s], row-major at offA[s]) is inverted in the precision mode of
+   sirocco_set_precision -- GSL-exactly in SIROCCO_FP64; in SIROCCO_FAST by the
+   certified kernel when N_s passes its M-matrix certificate, B and C then
+   formed inside that kernel -- and
    B_s = N_s^-1 diag(R_s) is written at offA[s] of B, with R_s the n[s] diagonal
    entries of R at offv[s].  C, which may be null, receives the row running
    totals of B (C[r][c] = B[r][0] + ... + B[r][c], summed left to right as

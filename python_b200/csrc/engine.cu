@@ -269,6 +269,7 @@ struct sirocco_plan {
   int* d_fboff = nullptr;
   int* d_fblist = nullptr;
   int* d_fbcount = nullptr;
+  ss::CertEpi epi;             // set only around a matom_matrices_batched run
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> ev;
   cudaEvent_t ev_fork = nullptr;
@@ -522,7 +523,8 @@ static int launch_bucket(const sirocco_plan* p, const Bucket& b, const double* A
   }
   if (b.fam == kFamCgj) {
     CertArgs ca{p->d_xcls, p->d_fboff, p->d_fblist, p->d_fbcount};
-    void* args[] = {&v, &ca};
+    CertEpi ep = p->epi;
+    void* args[] = {&v, &ca, &ep};
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -923,9 +925,13 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
   Context* c = ctx();
   int rc = c->init();
   if (rc) return rc;
+  // SIROCCO_FAST: certified inverses with the epilogue fused into their kernel;
+  // otherwise GSL-exact inverses followed by the epilogue kernel
+  const int md = (c->mode == SIROCCO_FAST) ? SIROCCO_FAST : SIROCCO_FP64;
   sirocco_plan* p = nullptr;
-  rc = c->get_plan(kInvert, nsys, n, offA, nullptr, SIROCCO_FP64, &p);
+  rc = c->get_plan(kInvert, nsys, n, offA, nullptr, md, &p);
   if (rc) return rc;
+  const bool fused = (md == SIROCCO_FAST);
   int64_t totV = 0;
   int maxn = 0;
   for (int s = 0; s < nsys; ++s) {
@@ -935,23 +941,51 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
   // blocks that fit 48 KB of shared memory are staged there (coalesced traffic)
   const size_t tile_bytes = sizeof(double) * size_t(maxn) * size_t(maxn);
   const bool tiled = tile_bytes <= size_t(48) << 10;
-  auto epilogue = [&](double* Bp, const double* Rp, double* Cp, const int* stp) -> int {
-    const int grid = std::max(1, std::min(nsys, p->num_sms * 16));
+  // the epilogue kernel over every system, or (fused) over the systems that
+  // the GSL-exact kernels served: their buckets' lists and the fallback lists
+  auto epilogue_on = [&](double* Bp, const double* Rp, double* Cp, const int* stp, EpiList el, int cnt) -> int {
+    const int grid = std::max(1, std::min(cnt, p->num_sms * 16));
+    const int64_t* dOv = static_cast<const int64_t*>(c->bOv.ptr);
     if (tiled)
-      matom_epilogue_tile_kernel<<<grid, 128, tile_bytes, c->stream>>>(nsys, p->d_n, p->d_offA,
-                                                                       static_cast<const int64_t*>(c->bOv.ptr), Bp,
-                                                                       Rp, Cp, stp);
+      matom_epilogue_tile_kernel<<<grid, 128, tile_bytes, c->stream>>>(nsys, p->d_n, p->d_offA, dOv, Bp, Rp, Cp, stp,
+                                                                       el);
     else
-      matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA,
-                                                         static_cast<const int64_t*>(c->bOv.ptr), Bp, Rp, Cp, stp);
+      matom_epilogue_kernel<<<grid, 128, 0, c->stream>>>(nsys, p->d_n, p->d_offA, dOv, Bp, Rp, Cp, stp, el);
     SS_CUDA(cudaGetLastError());
     return 0;
+  };
+  auto epilogue = [&](double* Bp, const double* Rp, double* Cp, const int* stp) -> int {
+    if (!fused) return epilogue_on(Bp, Rp, Cp, stp, EpiList{}, nsys);
+    for (const Bucket& b : p->buckets) {
+      if (b.fam == kFamCgj) continue;
+      EpiList el;
+      if (b.fb >= 0) {
+        el.list = p->d_fblist + p->fb_off[b.fb];
+        el.count_dev = p->d_fbcount + b.fb;
+      } else {
+        el.list = p->d_list + b.list_off;
+        el.count = b.count;
+      }
+      if (int r = epilogue_on(Bp, Rp, Cp, stp, el, b.count)) return r;
+    }
+    return 0;
+  };
+  // the plan run with the certified kernels writing B (and C) themselves
+  auto run_plan = [&](const double* Np, double* Bp, const double* Rp, double* Cp, int* stp) -> int {
+    if (fused) {
+      p->epi.offv = static_cast<const int64_t*>(c->bOv.ptr);
+      p->epi.R = Rp;
+      p->epi.C = Cp;
+    }
+    const int r = plan_run(p, Np, nullptr, Bp, stp, nullptr, c->stream);
+    p->epi = CertEpi{};
+    return r;
   };
   if ((rc = c->bOv.ensure(sizeof(int64_t) * size_t(nsys)))) return rc;
   int64_t* dOv = static_cast<int64_t*>(c->bOv.ptr);
   SS_CUDA(cudaMemcpyAsync(dOv, offv, sizeof(int64_t) * size_t(nsys), cudaMemcpyHostToDevice, c->stream));
   if (is_device_ptr(N)) {
-    rc = plan_run(p, N, nullptr, B, status, nullptr, c->stream);
+    rc = run_plan(N, B, R, C, status);
     if (rc) return rc;
     if ((rc = epilogue(B, R, C, status))) return rc;
     SS_CUDA(cudaStreamSynchronize(c->stream));
@@ -968,7 +1002,7 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
   int* dst = static_cast<int*>(c->bst.ptr);
   SS_CUDA(cudaMemcpyAsync(dN, N, bytesA, cudaMemcpyHostToDevice, c->stream));
   SS_CUDA(cudaMemcpyAsync(dR, R, bytesV, cudaMemcpyHostToDevice, c->stream));
-  rc = plan_run(p, dN, nullptr, dB, dst, nullptr, c->stream);
+  rc = run_plan(dN, dB, dR, dC, dst);
   if (rc) return rc;
   if ((rc = epilogue(dB, dR, dC, dst))) return rc;
   SS_CUDA(cudaMemcpyAsync(B, dB, bytesA, cudaMemcpyDeviceToHost, c->stream));

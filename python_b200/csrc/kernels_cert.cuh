@@ -90,6 +90,19 @@ struct CertArgs {
   int* fb_count;       // [classes] entries appended (zeroed before the launch)
 };
 
+// The macro-atom epilogue fused into the certified kernel (calc_matom_matrix,
+// source/macro_accelerate.c:325-334, and the running total of
+// matom_deactivation_from_matrix, :995-1008): with R set, the kernel writes
+// B = N^-1 diag(R) (one rounding per product, a_inverse * R as the reference
+// forms it) instead of N^-1, and with C set also the row running totals
+// C[r][c] = B[r][0] + ... + B[r][c], added left to right, one rounding per
+// addition.  R of system s starts at offv[s].
+struct CertEpi {
+  const int64_t* offv = nullptr;
+  const double* R = nullptr;
+  double* C = nullptr;
+};
+
 // P: padded order; WGR x WGC: tile-warp grid of one CTA; CL: CTAs per matrix (a
 // cluster); MINB: CTAs per SM asked of the register allocator.
 template <int P_, int WGR_, int WGC_, int CL_, int MINB_>
@@ -129,6 +142,8 @@ struct CgjShape {
   static_assert(SP % 2 == 0 && buf % 2 == 0 && off_dg % 2 == 0, "16-byte copies of the row panel");
   static_assert(LB <= 32, "one lane of the pivot warp issues each block's copy");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
+  static_assert(((LP + 31) / 32) * 32 * 33 <= off_dg && (LP + 31) / 32 <= NW,
+                "the running-total tiles fit the panel buffers, one tile warp per 32 rows");
 };
 
 __device__ __forceinline__ unsigned cluster_rank() {
@@ -220,7 +235,7 @@ __device__ __forceinline__ void warp_inv8(double& d0, double& d1, int lane) {
 
 template <int P, int WGR, int WGC, int CL, int MINB>
 __global__ void __launch_bounds__(32 * WGR * WGC + 32, MINB)
-cgj_inverse_kernel(BatchView bv, CertArgs ca) {
+cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
   using S = CgjShape<P, WGR, WGC, CL, MINB>;
   constexpr int NW = S::NW, NT = S::NT, WR = S::WR, WC = S::WC, LP = S::LP, LB = S::LB, CBK = S::CBK;
   constexpr int SP = S::SP, NBLK = P / 8;
@@ -583,9 +598,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
       }
     }
 
-    // ---- store N^-1
+    // ---- store N^-1, or B = N^-1 diag(R) with the fused epilogue
+    double* __restrict__ Og = bv.out + bv.offA[s];
     if (tile) {
-      double* __restrict__ Og = bv.out + bv.offA[s];
+      const double* __restrict__ Rs = ep.R ? ep.R + ep.offv[s] : nullptr;
 #pragma unroll
       for (int i = 0; i < WR; ++i) {
         const int r = grow(i);
@@ -595,8 +611,45 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca) {
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int c = gcol(j, e);
-              if (c < n) Og[int64_t(r) * n + c] = W[i][j][e];
+              if (c < n) Og[int64_t(r) * n + c] = Rs ? mul_rn(W[i][j][e], __ldg(Rs + c)) : W[i][j][e];
             }
+        }
+      }
+    }
+    if (ep.C) {
+      // running totals of each row this CTA holds, from the B just written (L2):
+      // a warp takes 32 local rows and walks them in 32 x 32 tiles, loaded and
+      // stored coalesced through shared memory (the panel buffers, free now),
+      // each lane adding its own row left to right as the reference does
+      __syncthreads();
+      double* __restrict__ Cg = ep.C + bv.offA[s];
+      constexpr int NG = (LP + 31) / 32;
+      if (tile && warp < NG) {
+        double* tl = sm + warp * (32 * 33);
+        auto row_of = [&](int lr) -> int {
+          return (lr < LP) ? ((((lr >> 3) * CL) + rank) * 8 + (lr & 7)) : n;
+        };
+        double total = 0.0;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+          const int c = c0 + lane;
+#pragma unroll 8
+          for (int k = 0; k < 32; ++k) {
+            const int rk = row_of(warp * 32 + k);
+            tl[k * 33 + lane] = (rk < n && c < n) ? __ldcg(Og + int64_t(rk) * n + c) : 0.0;
+          }
+          __syncwarp();
+          const int cm = min(32, n - c0);
+          for (int k = 0; k < cm; ++k) {
+            total = add_rn(total, tl[lane * 33 + k]);
+            tl[lane * 33 + k] = total;
+          }
+          __syncwarp();
+#pragma unroll 8
+          for (int k = 0; k < 32; ++k) {
+            const int rk = row_of(warp * 32 + k);
+            if (rk < n && c < n) Cg[int64_t(rk) * n + c] = tl[k * 33 + lane];
+          }
+          __syncwarp();
         }
       }
     }

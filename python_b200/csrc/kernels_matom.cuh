@@ -13,6 +13,20 @@
 
 namespace ss {
 
+// The systems an epilogue launch serves: all nsys of the batch, or the listed
+// ones (list[0 .. count), the count read from count_dev when that is set: a
+// list filled on the device by the certified kernel).
+struct EpiList {
+  const int* list = nullptr;
+  int count = 0;
+  const int* count_dev = nullptr;
+};
+__device__ __forceinline__ int epi_count(int nsys, const EpiList& el) {
+  if (!el.list) return nsys;
+  return el.count_dev ? *el.count_dev : el.count;
+}
+__device__ __forceinline__ int epi_system(int i, const EpiList& el) { return el.list ? el.list[i] : i; }
+
 // One CTA per system (grid-stride), one thread per row.  A singular system
 // (status != 0) gets B = 0 and C = 0: the reference's output of invert_matrix
 // is a zero-filled buffer that the failed call leaves untouched.
@@ -22,8 +36,10 @@ __global__ void __launch_bounds__(128) matom_epilogue_kernel(int nsys, const int
                                                              double* __restrict__ B,
                                                              const double* __restrict__ R,
                                                              double* __restrict__ C,
-                                                             const int* __restrict__ status) {
-  for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+                                                             const int* __restrict__ status, EpiList el) {
+  const int count = epi_count(nsys, el);
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const int s = epi_system(i, el);
     const int ns = n[s];
     const bool ok = status[s] == 0;
     double* __restrict__ Bs = B + offA[s];
@@ -52,9 +68,11 @@ __global__ void __launch_bounds__(128) matom_epilogue_tile_kernel(int nsys, cons
                                                                   double* __restrict__ B,
                                                                   const double* __restrict__ R,
                                                                   double* __restrict__ C,
-                                                                  const int* __restrict__ status) {
+                                                                  const int* __restrict__ status, EpiList el) {
   extern __shared__ double tile[];   // [n][n] of the current system
-  for (int s = blockIdx.x; s < nsys; s += gridDim.x) {
+  const int count = epi_count(nsys, el);
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const int s = epi_system(i, el);
     const int ns = n[s];
     const int nn = ns * ns;
     const bool ok = status[s] == 0;

@@ -215,10 +215,11 @@ def invert_batched(batch: Batch, mode: int = FP64, out: np.ndarray | None = None
     return out, st
 
 
-def matom_matrices(batch: Batch, R: np.ndarray, offv: np.ndarray, cumulative: bool = True):
+def matom_matrices(batch: Batch, R: np.ndarray, offv: np.ndarray, cumulative: bool = True, mode: int = FP64):
     """B = N^-1 diag(R) per cell and its row running totals through
-    matom_matrices_batched; returns (B, C or None, status)."""
+    matom_matrices_batched in precision mode `mode`; returns (B, C or None, status)."""
     lib = load()
+    set_precision(mode)
     n = np.ascontiguousarray(batch.n, np.int32)
     offv = np.ascontiguousarray(offv, np.int64)
     R = np.ascontiguousarray(R, np.float64)

@@ -25,10 +25,16 @@ def reference_walk(row_b, z):
 
 
 @pytest.mark.gpu
-def test_matom_matrices_match_inverse_times_r(engine):
+@pytest.mark.parametrize("mode", ["FP64", "FAST"])
+def test_matom_matrices_match_inverse_times_r(engine, mode):
+    """B equals the engine's own inverse in the same mode times R, bit for bit,
+    and C its left-to-right running totals; in SIROCCO_FAST the certified
+    kernel forms both itself (orders 33-216 here), the GSL-exact path and the
+    epilogue kernel the rest."""
+    m = getattr(engine, mode)
     batch, R, offv = wl.matom_cells(SIZES, seed=11)
-    B, C, st = engine.matom_matrices(batch, R, offv)
-    inv, sti = engine.invert_batched(batch)
+    B, C, st = engine.matom_matrices(batch, R, offv, mode=m)
+    inv, sti = engine.invert_batched(batch, m)
     ir, sr = oracle.invert(batch, "port", threads=oracle.host_threads())
     np.testing.assert_array_equal(st, sti)
     np.testing.assert_array_equal(st, sr)
@@ -48,13 +54,14 @@ def test_matom_matrices_match_inverse_times_r(engine):
 
 
 @pytest.mark.gpu
-def test_matom_singular_cell_gives_zero_matrices(engine):
+@pytest.mark.parametrize("mode", ["FP64", "FAST"])
+def test_matom_singular_cell_gives_zero_matrices(engine, mode):
     batch, R, offv = wl.matom_cells([12, 40], seed=3)
     m = batch.matrix(1).copy()
     m[7] = 0.0                       # a zero row: exactly singular
     mats = [batch.matrix(0), m]
     sb = wl.from_matrices("invert", mats)
-    B, C, st = engine.matom_matrices(sb, R, offv)
+    B, C, st = engine.matom_matrices(sb, R, offv, mode=getattr(engine, mode))
     _, sr = oracle.invert(sb, "port", threads=1)
     np.testing.assert_array_equal(st, sr)
     assert st[1] == 1 and st[0] == 0
