@@ -43,9 +43,10 @@
 // FP64 tensor-core MMA (mma.sync m8n8k4 f64: lane l holds row l/4, columns
 // 2(l%4) and 2(l%4)+1).  Each CTA also runs one pivot warp that holds no tile.
 // Every block step moves only the two panels through shared memory:
-//   S1  the warps holding K's rows write R (transposed, RowPT[c][q]); in a
-//       cluster the owner CTA's tile threads then copy that panel into every
-//       other CTA, 16 bytes per store; the warps holding K's columns write
+//   S1  the warps holding K's rows write R (transposed, RowPT[c][q]) into
+//       their CTA's shared memory, where the other CTAs of a cluster read
+//       their S3 operands (distributed shared memory); the warps holding K's
+//       columns write
 //       -C' (ColPN[r][q] = I - C on D's diagonal, -C elsewhere) locally; the
 //       holder of the next pivot block writes its current values (Dnext);
 //                                                               cluster barrier
@@ -139,7 +140,7 @@ struct CgjShape {
   static_assert(WGC * LP <= 2 * buf, "certificate partials fit the panel buffers");
   static_assert(CL >= 1 && CL <= 8, "portable cluster sizes");
   static_assert(off_stage % 2 == 0 && SLOT % 2 == 0, "16-byte aligned staging slots");
-  static_assert(SP % 2 == 0 && buf % 2 == 0 && off_dg % 2 == 0, "16-byte copies of the row panel");
+  static_assert(buf % 2 == 0 && off_dg % 2 == 0, "16-byte aligned buffers");
   static_assert(LB <= 32, "one lane of the pivot warp issues each block's copy");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
   static_assert(((LP + 31) / 32) * 32 * 33 <= off_dg && (LP + 31) / 32 <= NW,
@@ -312,29 +313,6 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
             }
         B[S::off_Dnext + g * SP + 2 * t] = v0;
         B[S::off_Dnext + g * SP + 2 * t + 1] = v1;
-      }
-    }
-  };
-
-  // cluster: the owner of block kblk copies its row panel into every other
-  // CTA once its tile threads have written it (a barrier over the tile threads
-  // only, so the pivot warp's work is not waited for), 16 bytes per store,
-  // consecutive threads on consecutive addresses
-  auto share_row_panel = [&](int kblk) {
-    if (CL > 1) {
-      asm volatile("bar.sync 1, %0;\n" ::"r"(NT) : "memory");
-      if (rank == kblk % CL) {
-        cg::cluster_group cl = cg::this_cluster();
-        const double2* src = reinterpret_cast<const double2*>(bufp(kblk) + S::off_RowPT);
-        for (int pr = 0; pr < CL; ++pr) {
-          if (pr == rank) continue;
-          double2* dst = reinterpret_cast<double2*>(cl.map_shared_rank(bufp(kblk) + S::off_RowPT, pr));
-          // the 8 values of each panel row, four 16-byte pieces, not the padding
-          for (int e = tid; e < 4 * P; e += NT) {
-            const int idx = (e >> 2) * (SP / 2) + (e & 3);
-            dst[idx] = src[idx];
-          }
-        }
       }
     }
   };
@@ -527,26 +505,24 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
     }
 
     // ---- prologue: the first panels (D(0)^-1 is already in place)
-    if (tile) {
-      publish(0);
-      share_row_panel(0);
-    }
+    if (tile) publish(0);
     cluster_barrier<CL>();
 
     // ---- blocked Gauss-Jordan, one 8 x 8 pivot block per step
     for (int kblk = 0; kblk < NBLK; ++kblk) {
       double* B = bufp(kblk);
+      // the row panel lives in the shared memory of the CTA that owns block
+      // kblk; the other CTAs of a cluster read its operands from there
       const double* RowPT = B + S::off_RowPT;
+      if (CL > 1 && rank != kblk % CL)
+        RowPT = cg::this_cluster().map_shared_rank(const_cast<double*>(RowPT), kblk % CL);
       double* RowNT = sm + S::off_RowNT;
       const double* ColP = B + S::off_ColP;
       const double* Dinv = B + S::off_Dinv;
       const int kb = 8 * kblk;
 
       if (kblk > 0) {
-        if (tile) {
-          publish(kblk);
-          share_row_panel(kblk);
-        }
+        if (tile) publish(kblk);
         cluster_barrier<CL>();   // also orders the pivot warp's D^-1 of this block
       }
 
@@ -620,8 +596,10 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
       // running totals of each row this CTA holds, from the B just written (L2):
       // a warp takes 32 local rows and walks them in 32 x 32 tiles, loaded and
       // stored coalesced through shared memory (the panel buffers, free now),
-      // each lane adding its own row left to right as the reference does
-      __syncthreads();
+      // each lane adding its own row left to right as the reference does.
+      // A cluster barrier first: the other CTAs may still be reading this
+      // CTA's row panel, in these buffers, for their last step.
+      cluster_barrier<CL>();
       double* __restrict__ Cg = ep.C + bv.offA[s];
       constexpr int NG = (LP + 31) / 32;
       if (tile && warp < NG) {
