@@ -86,7 +86,7 @@ constexpr int kCtaClasses = int(sizeof(kCtaP) / sizeof(kCtaP[0]));
 
 // padded orders of the certified Gauss-Jordan classes (cgj_classes.inc)
 static const int kCgjP[] = {
-#define SS_CGJ_CLASS(I, P, WGR, WGC, CL, MINB) P,
+#define SS_CGJ_CLASS(I, P, WGR, WGC, CL, MINB, ST) P,
 #include "cgj_classes.inc"
 #undef SS_CGJ_CLASS
 };
@@ -162,10 +162,10 @@ static KernelSpec cta_spec(int cls) {
 
 static KernelSpec cgj_spec(int cls) {
   KernelSpec k;
-#define SS_CGJ_CLASS(I, P, WGR, WGC, CL, MINB)                                       \
-  case I: {                                                                          \
-    using Sh = CgjShape<P, WGR, WGC, CL, MINB>;                                      \
-    k.fn = reinterpret_cast<const void*>(&cgj_inverse_kernel<P, WGR, WGC, CL, MINB>); \
+#define SS_CGJ_CLASS(I, P, WGR, WGC, CL, MINB, ST)                                      \
+  case I: {                                                                              \
+    using Sh = CgjShape<P, WGR, WGC, CL, MINB, ST>;                                      \
+    k.fn = reinterpret_cast<const void*>(&cgj_inverse_kernel<P, WGR, WGC, CL, MINB, ST>); \
     k.threads = Sh::NTH;                                                             \
     k.dyn_smem = Sh::dyn_smem;                                                       \
     k.cluster = CL;                                                                  \

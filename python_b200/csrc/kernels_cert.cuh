@@ -105,9 +105,12 @@ struct CertEpi {
 };
 
 // P: padded order; WGR x WGC: tile-warp grid of one CTA; CL: CTAs per matrix (a
-// cluster); MINB: CTAs per SM asked of the register allocator.
-template <int P_, int WGR_, int WGC_, int CL_, int MINB_>
+// cluster); MINB: CTAs per SM asked of the register allocator; STAGE: rows
+// arrive through the TMA staging slots (else straight from global memory into
+// registers, which leaves shared memory for more CTAs per SM).
+template <int P_, int WGR_, int WGC_, int CL_, int MINB_, bool STAGE_ = true>
 struct CgjShape {
+  static constexpr bool STAGE = STAGE_;
   static constexpr int P = P_, WGR = WGR_, WGC = WGC_, CL = CL_;
   static constexpr int NW = WGR * WGC;     // tile warps
   static constexpr int NT = 32 * NW;       // tile threads
@@ -133,7 +136,7 @@ struct CgjShape {
   static constexpr int off_bar = off_ok + 16;           // the staging mbarrier (8 bytes)
   static constexpr int SLOT = 8 * P + 2;                // doubles per staged 8-row block (+ alignment shift)
   static constexpr int off_stage = off_bar + 2;         // [LB][SLOT], 16-byte aligned
-  static constexpr int n_dbl = off_stage + LB * SLOT;
+  static constexpr int n_dbl = off_stage + (STAGE ? LB * SLOT : 0);
   static constexpr size_t dyn_smem = size_t(n_dbl) * 8;
   static_assert(P % (8 * CL) == 0 && LB % WGR == 0 && CBK % WGC == 0, "whole sub-block tiles");
   static_assert(NTH <= 1024, "one CTA");
@@ -141,7 +144,7 @@ struct CgjShape {
   static_assert(CL >= 1 && CL <= 8, "portable cluster sizes");
   static_assert(off_stage % 2 == 0 && SLOT % 2 == 0, "16-byte aligned staging slots");
   static_assert(buf % 2 == 0 && off_dg % 2 == 0, "16-byte aligned buffers");
-  static_assert(LB <= 32, "one lane of the pivot warp issues each block's copy");
+  static_assert(!STAGE || LB <= 32, "one lane of the pivot warp issues each block's copy");
   static_assert(dyn_smem <= 232448, "one CTA's shared memory");
   static_assert(((LP + 31) / 32) * 32 * 33 <= off_dg && (LP + 31) / 32 <= NW,
                 "the running-total tiles fit the panel buffers, one tile warp per 32 rows");
@@ -234,10 +237,10 @@ __device__ __forceinline__ void warp_inv8(double& d0, double& d1, int lane) {
   }
 }
 
-template <int P, int WGR, int WGC, int CL, int MINB>
+template <int P, int WGR, int WGC, int CL, int MINB, bool STAGE = true>
 __global__ void __launch_bounds__(32 * WGR * WGC + 32, MINB)
 cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
-  using S = CgjShape<P, WGR, WGC, CL, MINB>;
+  using S = CgjShape<P, WGR, WGC, CL, MINB, STAGE>;
   constexpr int NW = S::NW, NT = S::NT, WR = S::WR, WC = S::WC, LP = S::LP, LB = S::LB, CBK = S::CBK;
   constexpr int SP = S::SP, NBLK = P / 8;
   extern __shared__ __align__(16) double sm[];
@@ -388,7 +391,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
       if ((b1 & 15) && (ne > 1 || !shift)) slot[ne - 1] = tail_v;       // tail: b1 not 16-byte aligned
     }
   };
-  if (!tile) {
+  if (STAGE && !tile) {
     if (lane == 0) {
       mbar_init(bar, 1);
       asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -396,7 +399,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
     __syncwarp();
   }
   __syncthreads();
-  if (!tile && cid < cnt) stage_issue(cid);
+  if (STAGE && !tile && cid < cnt) stage_issue(cid);
   unsigned sphase = 0;
 
   int parity = 0;   // the certificate flags alternate buffers: a peer is at most one item ahead
@@ -406,34 +409,62 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
 
     // ---- this matrix's rows from the staging slots into registers (identity
     // padding), and the certificate's partial sums
-    const bool stalled = !mbar_wait(bar, sphase, kStageWaitPolls);
-    sphase ^= 1;
-    if (!tile && !stalled) stage_ends(s);
+    bool stalled = false;
+    if (STAGE) {
+      stalled = !mbar_wait(bar, sphase, kStageWaitPolls);
+      sphase ^= 1;
+      if (!tile && !stalled) stage_ends(s);
+    }
     __syncthreads();
     // the pivot warp of the CTA holding block 0 inverts D(0) straight from the
     // staging slots while the tile warps check the certificate (wasted, and
     // harmless, if the matrix fails it)
     if (!tile && rank == 0 && !stalled) {
-      uintptr_t b0, b1;
-      const int shift = block_span(s, 0, b0, b1) ? int((b0 >> 3) & 1) : 0;
-      const double* slot = stage + shift + g * n;
       double d[2];
+      if (STAGE) {
+        uintptr_t b0, b1;
+        const int shift = block_span(s, 0, b0, b1) ? int((b0 >> 3) & 1) : 0;
+        const double* slot = stage + shift + g * n;
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int c = 2 * t + e;
-        d[e] = (g < n && c < n) ? slot[c] : ((g == c) ? 1.0 : 0.0);
+        for (int e = 0; e < 2; ++e) {
+          const int c = 2 * t + e;
+          d[e] = (g < n && c < n) ? slot[c] : ((g == c) ? 1.0 : 0.0);
+        }
+      } else {
+        const double* Ag = bv.A + bv.offA[s];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int c = 2 * t + e;
+          d[e] = (g < n && c < n) ? __ldg(Ag + int64_t(g) * n + c) : ((g == c) ? 1.0 : 0.0);
+        }
       }
       pivot_inverse(0, d[0], d[1]);
     }
     double* red = sm;   // [WGC][LP] partial off-diagonal sums, over the panel buffers
     double* dg = sm + S::off_dg;
     bool zok = !stalled;
+    if (tile && !STAGE) {
+      // every load issued unconditionally (padding entries read A[0][0]), so
+      // all of a lane's loads are in flight at once
+      const double* __restrict__ Ag = bv.A + bv.offA[s];
+#pragma unroll
+      for (int i = 0; i < WR; ++i) {
+        const int r = grow(i);
+#pragma unroll
+        for (int j = 0; j < WC; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int c = gcol(j, e);
+            W[i][j][e] = __ldg(Ag + ((r < n && c < n) ? int64_t(r) * n + c : 0));
+          }
+      }
+    }
     if (tile) {
 #pragma unroll
       for (int i = 0; i < WR; ++i) {
         uintptr_t b0, b1;
         const int lb = wr + WGR * i;
-        const int shift = block_span(s, lb, b0, b1) ? int((b0 >> 3) & 1) : 0;
+        const int shift = (STAGE && block_span(s, lb, b0, b1)) ? int((b0 >> 3) & 1) : 0;
         const double* slot = stage + lb * S::SLOT + shift + g * n;
         const int r = grow(i);
         double part = 0.0;
@@ -442,7 +473,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const int c = gcol(j, e);
-            const double a = (r < n && c < n) ? slot[c] : ((r == c) ? 1.0 : 0.0);
+            const double a = (r < n && c < n) ? (STAGE ? slot[c] : W[i][j][e]) : ((r == c) ? 1.0 : 0.0);
             W[i][j][e] = a;
             if (c == r) {
               dg[lrow(i)] = a;
@@ -485,12 +516,12 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
       // a staging copy never completed: report it, give the copy a second
       // bounded wait, and leave (no CTA of the cluster issues more copies)
       if (rank == 0 && tid == 0) bv.status[s] = kStageTimeout;
-      if (stalled) mbar_wait(bar, sphase ^ 1, kStageWaitPolls);
+      if (STAGE && stalled) mbar_wait(bar, sphase ^ 1, kStageWaitPolls);
       cluster_barrier<CL>();
       return;
     }
     // the staging slots are free again: fetch the next matrix during this one
-    if (!tile && item + ncl < cnt) {
+    if (STAGE && !tile && item + ncl < cnt) {
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       stage_issue(item + ncl);
     }
