@@ -29,6 +29,7 @@
 
 #include "../../include/sirocco_solve.h"
 #include "kernels_cert.cuh"
+#include "kernels_certl.cuh"
 #include "kernels_cta.cuh"
 #include "kernels_global.cuh"
 #include "kernels_ionasm.cuh"
@@ -61,7 +62,7 @@ static void set_error(const char* fmt, ...) {
   } while (0)
 
 // ---------------------------------------------------------------- kernels --
-enum Family : int { kFamSmall = 0, kFamCta = 1, kFamGlobal = 2, kFamCgj = 3 };
+enum Family : int { kFamSmall = 0, kFamCta = 1, kFamGlobal = 2, kFamCgj = 3, kFamCgjL = 4 };
 
 struct KernelSpec {
   const void* fn = nullptr;
@@ -93,6 +94,9 @@ static const int kCgjP[] = {
 constexpr int kCgjClasses = int(sizeof(kCgjP) / sizeof(kCgjP[0]));
 // below this order the warp-group kernels of the exact path are faster
 constexpr int kCgjMinN = 33;
+// above the largest register-resident class, certified inverses stream
+// through global memory (kernels_certl.cuh), this many CTAs per SM
+constexpr int kCgjlMinB = 3;
 
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
@@ -179,6 +183,15 @@ static KernelSpec cgj_spec(int cls) {
   return k;
 }
 
+static KernelSpec cgjl_spec() {
+  using Sh = CgjlShape<kCgjlMinB>;
+  KernelSpec k;
+  k.fn = reinterpret_cast<const void*>(&cgjl_inverse_kernel<kCgjlMinB>);
+  k.threads = Sh::NTH;
+  k.dyn_smem = Sh::dyn_smem;
+  return k;
+}
+
 template <int KIND>
 static KernelSpec global_spec(int nmax) {
   KernelSpec k;
@@ -243,6 +256,7 @@ struct Bucket {
   int64_t scratch_off;
   int phase;      // 1: certified kernels and directly listed systems; 2: fallback lists
   int fb;         // phase 2: index of the fallback list this launch serves
+  int q;          // streamed certified inverses: index of the launch's queue counter
 };
 
 }  // namespace ss
@@ -264,6 +278,7 @@ struct sirocco_plan {
   bool own_scratch = true;     // false: d_scratch points into a pipeline's shared workspace
   // certified inverses: per system, the fallback list of its exact size class
   int nfb = 0;                 // fallback lists (exact classes that certified systems belong to)
+  int nq = 0;                  // queue counters (after the fallback counts in d_fbcount)
   std::vector<int> fb_off;     // start of each list in d_fblist
   int* d_xcls = nullptr;
   int* d_fboff = nullptr;
@@ -362,7 +377,7 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   // Certified inverses (SIROCCO_FAST) go to the Gauss-Jordan classes; each also
   // has a place in the fallback list of its exact class (small or CTA family).
   const bool cert = (kind == kInvert && mode == SIROCCO_FAST);
-  std::vector<int> small_l[8], cta_l[kCtaClasses], glob_l, cgj_l[kCgjClasses];
+  std::vector<int> small_l[8], cta_l[kCtaClasses], glob_l, cgj_l[kCgjClasses], cgjl_l;
   int small_fb[8] = {}, cta_fb[kCtaClasses] = {};
   for (int s = 0; s < nsys; ++s) {
     const int ns = n[s];
@@ -378,6 +393,11 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
       int e;
       if ((e = small_class(ns)) >= 0) small_fb[e]++;
       else cta_fb[cta_class(ns)]++;
+      continue;
+    }
+    if (cert && ns > kCgjP[kCgjClasses - 1]) {
+      cgjl_l.push_back(s);
+      cta_fb[cta_class(ns)]++;
       continue;
     }
     if ((c = small_class(ns)) >= 0) small_l[c].push_back(s);
@@ -404,11 +424,13 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
           const int e = small_class(n[s]);
           xcls[s] = (e >= 0) ? small_fbi[e] : cta_fbi[cta_class(n[s])];
         }
+      for (int s : cgjl_l) xcls[s] = cta_fbi[cta_class(n[s])];
       p->fb_off.push_back(off);   // total size of the lists
     }
   }
   // largest systems first within the global bucket (longest jobs start first)
   std::stable_sort(glob_l.begin(), glob_l.end(), [&](int x, int y) { return n[x] > n[y]; });
+  std::stable_sort(cgjl_l.begin(), cgjl_l.end(), [&](int x, int y) { return n[x] > n[y]; });
 
   std::vector<int> list;
   list.reserve(nsys);
@@ -425,7 +447,12 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
     b.fb = fb;
     b.list_off = int(list.size());
     if (l) list.insert(list.end(), l->begin(), l->end());
+    b.q = -1;
     if (fam == kFamCgj) b.spec = cgj_spec(cls);
+    else if (fam == kFamCgjL) {
+      b.spec = cgjl_spec();
+      b.q = p->nq++;
+    }
     else if (fam == kFamSmall) b.spec = (kind == kSolve) ? small_spec<kSolve>(cls, mode) : small_spec<kInvert>(cls, mode);
     else if (fam == kFamCta) b.spec = (kind == kSolve) ? cta_spec<kSolve>(cls) : cta_spec<kInvert>(cls);
     else b.spec = (kind == kSolve) ? global_spec<kSolve>(cls) : global_spec<kInvert>(cls);
@@ -451,6 +478,7 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   };
   int rc = 0;
   if (!glob_l.empty() && (rc = add_bucket(kFamGlobal, n[glob_l.front()], glob_l))) return rc;
+  if ((rc = add_bucket(kFamCgjL, 0, cgjl_l))) return rc;
   for (int c = kCgjClasses - 1; c >= 0; --c)
     if ((rc = add_bucket(kFamCgj, c, cgj_l[c]))) return rc;
   for (int c = kCtaClasses - 1; c >= 0; --c)
@@ -475,14 +503,16 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
       SS_CUDA(cudaMalloc(&p->d_offv, sizeof(int64_t) * nsys));
       SS_CUDA(cudaMemcpy(p->d_offv, offv, sizeof(int64_t) * nsys, cudaMemcpyHostToDevice));
     }
+    if (p->nfb + p->nq > 0) {
+      SS_CUDA(cudaMalloc(&p->d_fbcount, sizeof(int) * (p->nfb + p->nq)));
+      SS_CUDA(cudaMemset(p->d_fbcount, 0, sizeof(int) * (p->nfb + p->nq)));
+    }
     if (p->nfb > 0) {
       SS_CUDA(cudaMalloc(&p->d_xcls, sizeof(int) * nsys));
       SS_CUDA(cudaMemcpy(p->d_xcls, xcls.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice));
       SS_CUDA(cudaMalloc(&p->d_fboff, sizeof(int) * p->fb_off.size()));
       SS_CUDA(cudaMemcpy(p->d_fboff, p->fb_off.data(), sizeof(int) * p->fb_off.size(), cudaMemcpyHostToDevice));
       SS_CUDA(cudaMalloc(&p->d_fblist, sizeof(int) * std::max(1, p->fb_off.back())));
-      SS_CUDA(cudaMalloc(&p->d_fbcount, sizeof(int) * p->nfb));
-      SS_CUDA(cudaMemset(p->d_fbcount, 0, sizeof(int) * p->nfb));
     }
   }
   p->scratch_elems = scratch_elems;
@@ -521,7 +551,13 @@ static int launch_bucket(const sirocco_plan* p, const Bucket& b, const double* A
     v.list = p->d_fblist + p->fb_off[b.fb];
     v.count_dev = p->d_fbcount + b.fb;
   }
-  if (b.fam == kFamCgj) {
+  if (b.fam == kFamCgjL) {
+    CertArgs ca{p->d_xcls, p->d_fboff, p->d_fblist, p->d_fbcount};
+    CertEpi ep = p->epi;
+    int* queue = p->d_fbcount + p->nfb + b.q;
+    void* args[] = {&v, &ca, &ep, &queue};
+    SS_CUDA(cudaLaunchKernel(b.spec.fn, dim3(b.grid), dim3(b.spec.threads), args, b.spec.dyn_smem, st));
+  } else if (b.fam == kFamCgj) {
     CertArgs ca{p->d_xcls, p->d_fboff, p->d_fblist, p->d_fbcount};
     CertEpi ep = p->epi;
     void* args[] = {&v, &ca, &ep};
@@ -583,7 +619,7 @@ static int run_phase(sirocco_plan* p, int phase, const double* A, const double* 
 static int plan_run(sirocco_plan* p, const double* A, const double* bvec, double* out, int* status,
                     int* diag, cudaStream_t st) {
   if (p->buckets.empty()) return 0;
-  if (p->nfb > 0) SS_CUDA(cudaMemsetAsync(p->d_fbcount, 0, sizeof(int) * size_t(p->nfb), st));
+  if (p->nfb + p->nq > 0) SS_CUDA(cudaMemsetAsync(p->d_fbcount, 0, sizeof(int) * size_t(p->nfb + p->nq), st));
   int rc = run_phase(p, 1, A, bvec, out, status, diag, st);
   if (rc) return rc;
   return run_phase(p, 2, A, bvec, out, status, diag, st);
@@ -957,7 +993,7 @@ static int run_matom(int nsys, const int* n, const int64_t* offA, const int64_t*
   auto epilogue = [&](double* Bp, const double* Rp, double* Cp, const int* stp) -> int {
     if (!fused) return epilogue_on(Bp, Rp, Cp, stp, EpiList{}, nsys);
     for (const Bucket& b : p->buckets) {
-      if (b.fam == kFamCgj) continue;
+      if (b.fam == kFamCgj || b.fam == kFamCgjL) continue;
       EpiList el;
       if (b.fb >= 0) {
         el.list = p->d_fblist + p->fb_off[b.fb];
