@@ -101,6 +101,7 @@ def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:
         for p in CGJ_P:
             if n <= p:
                 return f"cgj{p}"
+        return "cgjl"   # streamed certified inverse, orders above the last class
     for np_ in (4, 8, 12, 16, 20, 24, 28, 32):
         if n <= np_:
             return f"small{np_}"
@@ -111,6 +112,8 @@ def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:
 
 
 def kernel_name(kind: str, cls: str, mode: str) -> str:
+    if cls == "cgjl":
+        return "cgjl_inverse_kernel"
     if cls.startswith("cgj"):
         return "cgj_inverse_kernel"
     if cls.startswith("small"):

@@ -95,8 +95,8 @@ constexpr int kCgjClasses = int(sizeof(kCgjP) / sizeof(kCgjP[0]));
 // below this order the warp-group kernels of the exact path are faster
 constexpr int kCgjMinN = 33;
 // above the largest register-resident class, certified inverses stream
-// through global memory (kernels_certl.cuh), this many CTAs per SM
-constexpr int kCgjlMinB = 3;
+// through global memory (kernels_certl.cuh): row tiles per pass, CTAs per SM
+constexpr int kCgjlRT = 1, kCgjlMinB = 3;
 
 static int small_class(int n) {
   for (int i = 0; i < 8; ++i)
@@ -184,9 +184,9 @@ static KernelSpec cgj_spec(int cls) {
 }
 
 static KernelSpec cgjl_spec() {
-  using Sh = CgjlShape<kCgjlMinB>;
+  using Sh = CgjlShape<kCgjlRT, kCgjlMinB>;
   KernelSpec k;
-  k.fn = reinterpret_cast<const void*>(&cgjl_inverse_kernel<kCgjlMinB>);
+  k.fn = reinterpret_cast<const void*>(&cgjl_inverse_kernel<kCgjlRT, kCgjlMinB>);
   k.threads = Sh::NTH;
   k.dyn_smem = Sh::dyn_smem;
   return k;

@@ -35,24 +35,31 @@
 
 namespace ss {
 
-template <int MINB_>
+// RT: 64-row tiles one pass updates against the same R' tile (4 warps each);
+// MINB: CTAs per SM asked of the register allocator
+template <int RT_, int MINB_>
 struct CgjlShape {
-  static constexpr int BT = 64;        // pivot columns per step; tile edge
-  static constexpr int NTH = 128;      // 4 warps, a 2 x 2 grid of 32 x 32 sub-tiles
-  static constexpr int SA = 68;        // shared tile row stride (doubles)
-  static constexpr int MINB = MINB_;   // CTAs per SM asked of the register allocator
-  static constexpr int off_A = 0;                 // [BT][SA] A operand: D^-1, or -W[I][K]
-  static constexpr int off_B = BT * SA;           // [BT][SA] B operand: W[K][J], or R'[K][J]
-  static constexpr int off_x = 2 * BT * SA;       // [2][BT] pivot row, [2][BT] pivot column
-  static constexpr int off_slot = off_x + 4 * BT; // queue item broadcast
+  static constexpr int RT = RT_;
+  static constexpr int BT = 64;          // pivot columns per step; tile edge
+  static constexpr int NTH = 128 * RT;   // 4 warps per row tile, a 2 x 2 grid of 32 x 32 sub-tiles
+  static constexpr int SA = 68;          // shared tile row stride (doubles)
+  static constexpr int MINB = MINB_;
+  static constexpr int off_A = 0;                   // [RT][BT][SA] A operands: D^-1, or -W[I][K]
+  static constexpr int off_B = RT * BT * SA;        // [BT][SA] B operand: W[K][J], or R'[K][J]
+  static constexpr int off_x = (RT + 1) * BT * SA;  // [2][BT] pivot row, [2][BT] pivot column
+  static constexpr int off_p = off_x + 4 * BT;      // [2] pivot reciprocals, by parity
+  static constexpr int off_slot = off_p + 2;        // queue item broadcast
   static constexpr int n_dbl = off_slot + 2;
   static constexpr size_t dyn_smem = size_t(n_dbl) * 8;
-  static_assert(4 * (32 * 33) <= 2 * BT * SA, "running-total tiles fit the operand buffers");
+  static_assert(RT == 1 || RT == 2, "one or two row tiles per pass");
+  static_assert((NTH / 32) * (32 * 33) <= (RT + 1) * BT * SA, "running-total tiles fit the operand buffers");
+  static_assert(dyn_smem <= 232448, "one CTA's shared memory");
 };
 
 namespace cgjl {
 
 constexpr int BT = 64, SA = 68;
+using Acc = double[4][4][2];
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -61,29 +68,88 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // tile [r0, r0 + rb) x [c0, c0 + cb) of an n x n row-major matrix into a BT x BT
-// shared tile, zero outside (identity on the diagonal when ident), negated
-// when neg
-__device__ __forceinline__ void load_tile(double* __restrict__ dst, const double* src, int n, int r0, int rb,
-                                          int c0, int cb, bool ident, bool neg, int tid) {
-  double v[32];
+// shared tile, zero outside, negated when neg; NTH threads
+template <int NTH>
+__device__ __forceinline__ void load_tile(double* __restrict__ dst, const double* src, int n, int r0, int rb, int c0,
+                                          int cb, bool neg, int tid) {
+  constexpr int PER = BT * BT / NTH;
+  double v[PER];
 #pragma unroll
-  for (int m = 0; m < 32; ++m) {
-    const int e = tid + 128 * m, r = e >> 6, c = e & 63;
+  for (int m = 0; m < PER; ++m) {
+    const int e = tid + NTH * m, r = e >> 6, c = e & 63;
     v[m] = (r < rb && c < cb) ? src[int64_t(r0 + r) * n + c0 + c] : 0.0;
   }
 #pragma unroll
-  for (int m = 0; m < 32; ++m) {
-    const int e = tid + 128 * m, r = e >> 6, c = e & 63;
-    double x = neg ? -v[m] : v[m];
-    if (ident) x = (r == c && r < rb) ? 1.0 : 0.0;
-    dst[r * SA + c] = x;
+  for (int m = 0; m < PER; ++m) {
+    const int e = tid + NTH * m, r = e >> 6, c = e & 63;
+    dst[r * SA + c] = neg ? -v[m] : v[m];
+  }
+}
+
+template <int NTH>
+__device__ __forceinline__ void identity_tile(double* __restrict__ dst, int rb, int tid) {
+#pragma unroll
+  for (int m = 0; m < BT * BT / NTH; ++m) {
+    const int e = tid + NTH * m, r = e >> 6, c = e & 63;
+    dst[r * SA + c] = (r == c && r < rb) ? 1.0 : 0.0;
+  }
+}
+
+// a warp's 32 x 32 part of tile [r0 ..) x [c0 ..) in accumulator layout (lane:
+// rows 8 i + g, columns 8 j + 2 t and + 1), zero outside or when zero; vec:
+// rows start 16-byte aligned and n is even (each pair in or out together)
+__device__ __forceinline__ void load_acc(Acc& acc, const double* src, int n, int r0, int rb, int c0, int cb,
+                                         bool zero, bool vec, int wr, int wc, int g, int t) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = 32 * wr + 8 * i + g;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = 32 * wc + 8 * j + 2 * t;
+      const double* a = src + int64_t(r0 + r) * n + c0 + c;
+      if (vec) {
+        const bool ok = !zero && r < rb && c < cb;
+        const double2 v = ok ? *reinterpret_cast<const double2*>(a) : make_double2(0.0, 0.0);
+        acc[i][j][0] = v.x;
+        acc[i][j][1] = v.y;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) acc[i][j][e] = (!zero && r < rb && c + e < cb) ? a[e] : 0.0;
+      }
+    }
+  }
+}
+
+// the same part written back, each entry times R[c0 + c] when R is set
+__device__ __forceinline__ void store_acc(const Acc& acc, double* dst, int n, int r0, int rb, int c0, int cb,
+                                          const double* __restrict__ R, bool vec, int wr, int wc, int g, int t) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = 32 * wr + 8 * i + g;
+    if (r >= rb) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = 32 * wc + 8 * j + 2 * t;
+      double* a = dst + int64_t(r0 + r) * n + c0 + c;
+      double v0 = acc[i][j][0], v1 = acc[i][j][1];
+      if (R) {
+        if (c < cb) v0 = mul_rn(v0, __ldg(R + c0 + c));
+        if (c + 1 < cb) v1 = mul_rn(v1, __ldg(R + c0 + c + 1));
+      }
+      if (vec) {
+        if (c < cb) *reinterpret_cast<double2*>(a) = make_double2(v0, v1);
+      } else {
+        if (c < cb) a[0] = v0;
+        if (c + 1 < cb) a[1] = v1;
+      }
+    }
   }
 }
 
 // acc += A B over the 64-deep tiles: warp (wr, wc) covers rows 32 wr .. +32,
 // columns 32 wc .. +32 in 4 x 4 fragments
-__device__ __forceinline__ void mma_tile(double (&acc)[4][4][2], const double* __restrict__ As,
-                                         const double* __restrict__ Bs, int wr, int wc, int g, int t) {
+__device__ __forceinline__ void mma_tile(Acc& acc, const double* __restrict__ As, const double* __restrict__ Bs,
+                                         int wr, int wc, int g, int t) {
 #pragma unroll 4
   for (int kk = 0; kk < BT / 4; ++kk) {
     double a[4], b[4];
@@ -98,13 +164,45 @@ __device__ __forceinline__ void mma_tile(double (&acc)[4][4][2], const double* _
   }
 }
 
+// the same over a tile whose last rows, columns or depth are padding: only
+// the kq 4-deep slices and this warp's ni x nj sub-blocks that hold data
+__device__ __forceinline__ void mma_tile_edge(Acc& acc, const double* __restrict__ As,
+                                              const double* __restrict__ Bs, int wr, int wc, int g, int t, int kq,
+                                              int ni, int nj) {
+  for (int kk = 0; kk < kq; ++kk) {
+    double a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = (i < ni) ? As[(32 * wr + 8 * i + g) * SA + 4 * kk + t] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = (j < nj) ? Bs[(4 * kk + t) * SA + 32 * wc + 8 * j + g] : 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (i < ni && j < nj) dmma_884(acc[i][j], a[i], b[j]);
+  }
+}
+
+// acc += A B for a tile of rb rows, cb columns and depth kb
+__device__ __forceinline__ void mma_any(Acc& acc, const double* __restrict__ As, const double* __restrict__ Bs,
+                                        int wr, int wc, int g, int t, int rb, int cb, int kb) {
+  if (rb == BT && cb == BT && kb == BT) {
+    mma_tile(acc, As, Bs, wr, wc, g, t);
+  } else {
+    const int ni = min(4, max(0, (rb - 32 * wr + 7) >> 3)), nj = min(4, max(0, (cb - 32 * wc + 7) >> 3));
+    if (ni > 0 && nj > 0) mma_tile_edge(acc, As, Bs, wr, wc, g, t, (kb + 3) >> 2, ni, nj);
+  }
+}
+
 }  // namespace cgjl
 
-template <int MINB>
-__global__ void __launch_bounds__(128, MINB)
+template <int RT, int MINB>
+__global__ void __launch_bounds__(128 * RT, MINB)
     cgjl_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep, int* __restrict__ queue) {
   using namespace cgjl;
-  using S = CgjlShape<MINB>;
+  using S = CgjlShape<RT, MINB>;
+  constexpr int NTH = S::NTH, NWARP = NTH / 32;
+  constexpr int RPT = BT / (NTH / 64);   // rows of the pivot block per thread in the D^-1 phase
   extern __shared__ __align__(16) double sm[];
   double* As = sm + S::off_A;
   double* Bs = sm + S::off_B;
@@ -113,7 +211,9 @@ __global__ void __launch_bounds__(128, MINB)
   int* slot = reinterpret_cast<int*>(sm + S::off_slot);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int wr = warp >> 1, wc = warp & 1;
+  const int rt = warp >> 2;                       // the row tile of this warp's pass
+  const int wr = (warp >> 1) & 1, wc = warp & 1;  // its 32 x 32 part
+  const double* Ao = As + rt * (BT * SA);         // its A operand
   const int cnt = batch_count(bv);
 
   for (;;) {
@@ -126,21 +226,30 @@ __global__ void __launch_bounds__(128, MINB)
     const int n = bv.n[s];
     const double* Ag = bv.A + bv.offA[s];
     double* Wg = bv.out + bv.offA[s];
+    const bool vA = ((n & 1) == 0) && ((reinterpret_cast<uintptr_t>(Ag) & 15) == 0);
+    const bool vW = ((n & 1) == 0) && ((reinterpret_cast<uintptr_t>(Wg) & 15) == 0);
 
-    // ---- certificate, a warp per row (coalesced)
+    // ---- certificate, a warp per row, all of a row's loads in flight at once
     bool ok = true;
-    for (int r = warp; r < n; r += 4) {
+    for (int r = warp; r < n; r += NWARP) {
       const double* row = Ag + int64_t(r) * n;
+      double v[32];
+#pragma unroll
+      for (int u = 0; u < 32; ++u) {
+        const int c = lane + 32 * u;
+        v[u] = (c < n) ? row[c] : 0.0;
+      }
+      const double d = row[r];
       double off = 0.0;
-      for (int c = lane; c < n; c += 32) {
-        const double a = row[c];
+#pragma unroll
+      for (int u = 0; u < 32; ++u) {
+        const int c = lane + 32 * u;
         if (c != r) {
-          ok &= (a <= 0.0);   // false for NaN
-          off += fabs(a);
+          ok &= (v[u] <= 0.0);   // false for NaN
+          off += fabs(v[u]);
         }
       }
       off = warp_sum(off);
-      const double d = row[r];
       ok &= (d > 0.0) && (d < INFINITY) && (off * (1.0 + 0x1p-40) <= (1.0 - kCertMargin) * d);
     }
     if (!__syncthreads_and(int(ok))) {
@@ -156,117 +265,114 @@ __global__ void __launch_bounds__(128, MINB)
     for (int kt = 0; kt < nb; ++kt) {
       const int k0 = kt * BT, kb = min(BT, n - k0);
       const double* src = (kt == 0) ? Ag : Wg;   // the first step reads the input
+      const bool vs = (kt == 0) ? vA : vW;
 
-      // ---- D^-1: thread (column c, rows 32 h ..) of the padded 64 x 64 block
+      // ---- D^-1 into As[0]: thread (column c, rows RPT h ..) of the padded block
       {
         const int c = tid & 63, h = tid >> 6;
-        double dv[32];
+        double dv[RPT];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          const int r = 32 * h + i;
+        for (int i = 0; i < RPT; ++i) {
+          const int r = RPT * h + i;
           dv[i] = (r < kb && c < kb) ? src[int64_t(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
         }
+        double* px = sm + S::off_p;
+        // pivot j = RPT jh + jj: the holder of the pivot entry forms its
+        // reciprocal once; the holders of row j and column j publish them
+        for (int jh = 0; jh < BT / RPT; ++jh) {
 #pragma unroll
-        for (int j = 0; j < BT; ++j) {
-          double* rx = xr + (j & 1) * BT;
-          double* cx = xc + (j & 1) * BT;
-          if (h == (j >> 5)) rx[c] = dv[j & 31];
-          if (c == j) {
+          for (int jj = 0; jj < RPT; ++jj) {
+            const int j = RPT * jh + jj, par = jj & 1;
+            double* rx = xr + par * BT;
+            double* cx = xc + par * BT;
+            if (h == jh) {
+              rx[c] = dv[jj];
+              if (c == j) px[par] = 1.0 / dv[jj];
+            }
+            if (c == j) {
 #pragma unroll
-            for (int i = 0; i < 32; ++i) cx[32 * h + i] = dv[i];
-          }
-          __syncthreads();
-          const double p = 1.0 / rx[j];
-          const double rj = rx[c] * p;
+              for (int i = 0; i < RPT; ++i) cx[RPT * h + i] = dv[i];
+            }
+            __syncthreads();
+            const double p = px[par];
+            const double rj = rx[c] * p;
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            const int r = 32 * h + i;
-            if (r == j) {
-              dv[i] = (c == j) ? p : rj;
-            } else {
-              const double f = cx[r];
-              dv[i] = (c == j) ? -f * p : fma(-f, rj, dv[i]);
+            for (int i = 0; i < RPT; ++i) {
+              if (h == jh && i == jj) {
+                dv[i] = (c == j) ? p : rj;
+              } else {
+                const double f = cx[RPT * h + i];
+                dv[i] = (c == j) ? -f * p : fma(-f, rj, dv[i]);
+              }
             }
           }
         }
 #pragma unroll
-        for (int i = 0; i < 32; ++i) As[(32 * h + i) * SA + c] = dv[i];
+        for (int i = 0; i < RPT; ++i) As[(RPT * h + i) * SA + c] = dv[i];
       }
 
-      // ---- R' = D^-1 W[K][J] on the pivot rows (D^-1 on K's own tile)
-      for (int jt = 0; jt < nb; ++jt) {
-        const int j0 = jt * BT, jb = min(BT, n - j0);
-        load_tile(Bs, src, n, k0, kb, j0, jb, jt == kt, false, tid);
-        __syncthreads();
-        double acc[4][4][2];
+      // ---- R' = D^-1 W[K][J] on the pivot rows (D^-1 on K's own tile); with
+      // two row groups, the second takes tile J + 1 with its B operand in As[1]
+      for (int jt = 0; jt < nb; jt += RT) {
+        __syncthreads();   // D^-1 written / the previous tiles' operands read
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-        mma_tile(acc, As, Bs, wr, wc, g, t);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int r = 32 * wr + 8 * i + g;
-          if (r < kb) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                const int c = 32 * wc + 8 * j + 2 * t + e;
-                if (c < jb) Wg[int64_t(k0 + r) * n + j0 + c] = acc[i][j][e];
-              }
+        for (int q = 0; q < RT; ++q) {
+          const int jq = jt + q;
+          double* Bq = (q == 0) ? Bs : As + BT * SA;
+          if (jq < nb) {
+            if (jq == kt) identity_tile<NTH>(Bq, kb, tid);
+            else load_tile<NTH>(Bq, src, n, k0, kb, jq * BT, min(BT, n - jq * BT), false, tid);
           }
         }
         __syncthreads();
+        const int jq = jt + rt;
+        if (jq < nb) {
+          Acc acc;
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+          mma_any(acc, As, (rt == 0) ? Bs : As + BT * SA, wr, wc, g, t, kb, min(BT, n - jq * BT), kb);
+          // the pivot rows stay unscaled by R until no tile reads them
+          store_acc(acc, Wg, n, k0, kb, jq * BT, min(BT, n - jq * BT), nullptr, vW, wr, wc, g, t);
+        }
       }
+      __syncthreads();
 
-      // ---- every other row tile: W[I][:] += (-W[I][K]) R'
+      // ---- the other row tiles, RT per pass: W[I][:] += (-W[I][K]) R'
       const bool last = (kt == nb - 1);
       const double* __restrict__ Rs = (last && ep.R) ? ep.R + ep.offv[s] : nullptr;
-      for (int it = 0; it < nb; ++it) {
-        if (it == kt) continue;
-        const int i0 = it * BT, ib = min(BT, n - i0);
-        load_tile(As, src, n, i0, ib, k0, kb, false, true, tid);
+      for (int ip = 0; ip < nb - 1; ip += RT) {
+        // pass rows: the ip-th .. other-than-K row tiles
+        auto tile_row = [&](int u) { return u + (u >= kt); };
+#pragma unroll
+        for (int q = 0; q < RT; ++q) {
+          const int u = ip + q;
+          if (u < nb - 1) {
+            const int i0 = tile_row(u) * BT;
+            load_tile<NTH>(As + q * (BT * SA), src, n, i0, min(BT, n - i0), k0, kb, true, tid);
+          }
+        }
+        const int u = ip + rt;
+        const bool act = u < nb - 1;
+        const int i0 = act ? tile_row(u) * BT : 0, ib = act ? min(BT, n - i0) : 0;
         for (int jt = 0; jt < nb; ++jt) {
           const int j0 = jt * BT, jb = min(BT, n - j0);
           // the tile's own values first (HBM), then R' (L2): both in flight at once
-          double acc[4][4][2];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int r = 32 * wr + 8 * i + g;
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                const int c = 32 * wc + 8 * j + 2 * t + e;
-                acc[i][j][e] = (jt != kt && r < ib && c < jb) ? src[int64_t(i0 + r) * n + j0 + c] : 0.0;
-              }
-          }
-          load_tile(Bs, Wg, n, k0, kb, j0, jb, false, false, tid);
+          Acc acc;
+          load_acc(acc, src, n, i0, ib, j0, jb, jt == kt || !act, vs, wr, wc, g, t);
+          load_tile<NTH>(Bs, Wg, n, k0, kb, j0, jb, false, tid);
           __syncthreads();
-          mma_tile(acc, As, Bs, wr, wc, g, t);
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int r = 32 * wr + 8 * i + g;
-            if (r < ib) {
-#pragma unroll
-              for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                  const int c = 32 * wc + 8 * j + 2 * t + e;
-                  if (c < jb) {
-                    const double w = acc[i][j][e];
-                    Wg[int64_t(i0 + r) * n + j0 + c] = Rs ? mul_rn(w, __ldg(Rs + j0 + c)) : w;
-                  }
-                }
-            }
+          if (act) {
+            mma_any(acc, Ao, Bs, wr, wc, g, t, ib, jb, kb);
+            store_acc(acc, Wg, n, i0, ib, j0, jb, Rs, vW, wr, wc, g, t);
           }
           __syncthreads();
         }
       }
       // the pivot rows of the last step, scaled now that no tile reads them
       if (Rs) {
-        for (int e = tid; e < kb * n; e += S::NTH) {
+        for (int e = tid; e < kb * n; e += NTH) {
           const int r = e / n, c = e - r * n;
           double* w = Wg + int64_t(k0 + r) * n + c;
           *w = mul_rn(*w, __ldg(Rs + c));
@@ -280,7 +386,7 @@ __global__ void __launch_bounds__(128, MINB)
     if (ep.C) {
       double* __restrict__ Cg = ep.C + bv.offA[s];
       double* tl = sm + warp * (32 * 33);
-      for (int r0 = 32 * warp; r0 < n; r0 += 128) {
+      for (int r0 = 32 * warp; r0 < n; r0 += 32 * NWARP) {
         double total = 0.0;
         for (int c0 = 0; c0 < n; c0 += 32) {
           const int c = c0 + lane;

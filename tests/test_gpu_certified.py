@@ -3,8 +3,10 @@
 Matrices that pass the certificate (nonsingular M-matrices with a relative
 row-dominance margin of at least 1e-5) are inverted by Gauss-Jordan without
 pivoting: code 0, as GSL's, and the inverse within 1e-10 (max-abs, relative to
-the largest entry) of the reference build's.  Every other matrix falls back to
-the GSL-exact path, whose results must equal SIROCCO_FP64 mode's bit for bit.
+the largest entry) of the reference build's.  Orders 33-216 run the
+register-resident kernel, orders 217-1024 the streamed one.  Every other
+matrix falls back to the GSL-exact path, whose results must equal
+SIROCCO_FP64 mode's bit for bit.
 """
 import numpy as np
 import pytest
@@ -62,6 +64,63 @@ def test_certified_every_class_matches_gsl(engine, lo, hi):
     assert (diag == CERTIFIED_DIAG).all()
     err = per_system_err(inv, ir, batch)
     assert err.max() <= INV_TOL, (batch.n[np.argmax(err)], err.max())
+
+
+# the streamed kernel: 64-column steps, so the orders around multiples of 64
+# (partial last tiles and steps) and both ends of its range
+STREAMED_ORDERS = [217, 230, 255, 256, 257, 300, 319, 320, 321, 383, 384, 449, 511, 512, 513, 640, 700, 777,
+                   895, 960, 1000, 1023, 1024]
+
+
+def test_certified_streamed_orders_match_gsl(engine):
+    batch = wl.macro_batch(STREAMED_ORDERS, seed=217, density=0.10)
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    assert (diag == CERTIFIED_DIAG).all()
+    err = per_system_err(inv, ir, batch)
+    assert err.max() <= INV_TOL, (batch.n[np.argmax(err)], err.max())
+
+
+def test_certified_streamed_fallback_and_odd_layout(engine):
+    """Streamed orders that fail the certificate take the exact path (bit-equal
+    to SIROCCO_FP64); the good ones are inverted at offsets that leave their
+    rows 8-byte but not 16-byte aligned (an odd number of doubles before each)."""
+    rng = np.random.default_rng(23)
+    good = [wl.macro_matrix(rng, int(n), density=0.10) for n in (218, 260, 402, 514)]
+    bad = []
+    m = wl.macro_matrix(rng, 300, density=0.10)
+    m[17, 40] = 2e-3                            # a positive off-diagonal entry
+    bad.append(m)
+    m = wl.macro_matrix(rng, 600, density=0.10)
+    m[100, :] = 0.0                             # singular: the reference returns 1
+    bad.append(m)
+    m = wl.macro_matrix(rng, 257, density=0.10)
+    m[3, 3] = np.inf
+    bad.append(m)
+    mats = [good[0], bad[0], good[1], bad[1], good[2], bad[2], good[3]]
+    n = np.array([x.shape[0] for x in mats], dtype=np.int32)
+    offA = np.zeros(len(mats), dtype=np.int64)
+    pos = 1                                     # every matrix starts at an odd element offset
+    for s, x in enumerate(mats):
+        offA[s] = pos
+        pos += x.size + (1 if (pos + x.size) % 2 == 0 else 0)
+    A = np.zeros(pos, dtype=np.float64)
+    for s, x in enumerate(mats):
+        A[offA[s]:offA[s] + x.size] = x.ravel()
+    batch = wl.Batch("invert", n, offA, A)
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    inv64, st64, _ = run_plan(engine, batch, engine.FP64)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    np.testing.assert_array_equal(st, st64)
+    fb = (diag & (1 << 8)) != 0
+    assert fb.tolist() == [False, True, False, True, False, True, False]
+    for s in np.nonzero(fb)[0]:
+        o, k = int(offA[s]), int(n[s])
+        assert same_values(inv[o:o + k * k], inv64[o:o + k * k]).all(), s
+    err = per_system_err(inv, ir, batch)
+    assert err[~fb].max() <= INV_TOL
 
 
 def test_certified_config3_macro_sample(engine):
@@ -132,6 +191,7 @@ def test_certified_plan_in_a_cuda_graph(engine):
     import torch
     rng = np.random.default_rng(5)
     mats = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 217, 300)]
+    mats += [wl.macro_matrix(rng, int(n), density=0.10) for n in (230, 333, 480)]   # the streamed kernel's queue
     bad = uncertified_matrices(rng)
     batch = wl.from_matrices("invert", mats[:150] + bad + mats[150:])
     want, wst, _ = run_plan(engine, batch, engine.FAST)
