@@ -677,7 +677,7 @@ struct Pipeline {
 };
 
 #ifndef SS_CHUNK_MIB
-#define SS_CHUNK_MIB 16   // host pipeline chunk size
+#define SS_CHUNK_MIB 16   // smallest host pipeline chunk
 #endif
 #ifndef SS_PIPE_STREAMS
 #define SS_PIPE_STREAMS 4 // host pipeline streams
@@ -687,18 +687,32 @@ constexpr size_t kPlanCache = 16;                      // plans cached per threa
 constexpr int64_t kPlanWorkBytes = int64_t(8) << 30;   // workspace the cached plans may hold
 constexpr int64_t kChunkBytes = int64_t(SS_CHUNK_MIB) << 20;
 
-// host pipeline chunk size: SIROCCO_CHUNK_MIB overrides the built-in size (read once)
-static int64_t chunk_bytes() {
-  static const int64_t v = [] {
+constexpr int kPipeChunks = 12;                        // chunks a large batch is cut into
+constexpr int kChunkSysPerSM = 4;                      // systems per SM a chunk holds at least
+constexpr int64_t kMaxChunkBytes = int64_t(4) << 30;
+
+// Host pipeline chunk size for a batch of `total` bytes and nsys systems:
+// about a twelfth of the batch, but at least the bytes of 4 systems per SM
+// (of the batch's average size) so that every chunk's launch still fills the
+// GPU, within [SS_CHUNK_MIB, 4 GiB].  Copies of the other chunks overlap a
+// chunk's kernels.  (Config-4-like batches, 2,048 matrices of order 256-1024:
+// 16 MiB chunks hold two or three matrices and ran at 660 systems/s end to end;
+// chunks of a twelfth, 4,800/s; of a quarter, 8,300/s.)  SIROCCO_CHUNK_MIB
+// fixes the size instead (read once).
+static int64_t chunk_bytes(int64_t total, int nsys, int sms) {
+  static const int64_t fixed = [] {
     const char* e = std::getenv("SIROCCO_CHUNK_MIB");
     const long m = e ? std::strtol(e, nullptr, 10) : 0;
-    return (m > 0 && m <= 4096) ? int64_t(m) << 20 : kChunkBytes;
+    return (m > 0 && m <= 4096) ? int64_t(m) << 20 : int64_t(0);
   }();
-  return v;
+  if (fixed > 0) return fixed;
+  const int64_t fill = nsys > 0 ? total / nsys * kChunkSysPerSM * sms : 0;
+  return std::min(kMaxChunkBytes, std::max({kChunkBytes, total / kPipeChunks, fill}));
 }
 
 struct Context {
   int device = -1;
+  int num_sms = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t pipe[kPipeStreams] = {};
   cudaEvent_t pipe_ev[kPipeStreams] = {};
@@ -734,6 +748,7 @@ struct Context {
     if (device == dev && stream) return 0;
     release();
     SS_CUDA(cudaSetDevice(dev));
+    SS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
     SS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (int i = 0; i < kPipeStreams; ++i) {
       SS_CUDA(cudaStreamCreateWithFlags(&pipe[i], cudaStreamNonBlocking));
@@ -753,11 +768,13 @@ struct Context {
     }
     std::unique_ptr<Pipeline> pl(new Pipeline());
     std::vector<int64_t> ra, rv;
+    const int64_t cb = chunk_bytes(nsys > 0 ? 8 * (offA[nsys - 1] + int64_t(n[nsys - 1]) * n[nsys - 1] - offA[0]) : 0,
+                                   nsys, num_sms);
     int s0 = 0;
     while (s0 < nsys) {
       int s1 = s0;
       int64_t bytes = 0;
-      while (s1 < nsys && (s1 == s0 || bytes < chunk_bytes())) {
+      while (s1 < nsys && (s1 == s0 || bytes < cb)) {
         bytes += int64_t(n[s1]) * n[s1] * 8;
         ++s1;
       }
@@ -899,7 +916,7 @@ static int run_batched(int kind, int nsys, const int* n, const int64_t* offA, co
   for (int s = 0; s + 1 < nsys && packed; ++s) {
     packed = offA[s + 1] == offA[s] + int64_t(n[s]) * n[s] && (kind != kSolve || offv[s + 1] == offv[s] + n[s]);
   }
-  if (packed && bytesA > size_t(2 * chunk_bytes())) {
+  if (packed && bytesA > size_t(2 * chunk_bytes(int64_t(bytesA), nsys, c->num_sms))) {
     // chunked pipeline: the copies of one chunk overlap the kernels of the others
     Pipeline* pl = nullptr;
     rc = c->get_pipeline(kind, nsys, n, offA, kind == kSolve ? offv : nullptr, md, &pl);
