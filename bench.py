@@ -92,7 +92,7 @@ def make_batches(config: int, nsys: int | None = None):
     raise SystemExit(f"unknown config {config}")
 
 
-CGJ_P = (40, 48, 56, 64, 80, 96, 112, 128, 144, 160, 176, 192, 216)   # csrc/cgj_classes.inc
+CGJ_P = (40, 48, 56, 64, 80, 96, 112, 128, 144, 160, 176, 192, 208, 224)   # csrc/cgj_classes.inc
 
 
 def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:

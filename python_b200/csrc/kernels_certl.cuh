@@ -1,4 +1,4 @@
-// Certified inverse for orders above the register-resident classes (217 ..
+// Certified inverse for orders above the register-resident classes (225 ..
 // 1024): blocked Gauss-Jordan without pivoting, streamed through global
 // memory, its updates on the FP64 tensor-core MMA.
 //

@@ -3,8 +3,8 @@
 Matrices that pass the certificate (nonsingular M-matrices with a relative
 row-dominance margin of at least 1e-5) are inverted by Gauss-Jordan without
 pivoting: code 0, as GSL's, and the inverse within 1e-10 (max-abs, relative to
-the largest entry) of the reference build's.  Orders 33-216 run the
-register-resident kernel, orders 217-1024 the streamed one.  Every other
+the largest entry) of the reference build's.  Orders 33-224 run the
+register-resident kernel, orders 225-1024 the streamed one.  Every other
 matrix falls back to the GSL-exact path, whose results must equal
 SIROCCO_FP64 mode's bit for bit.
 """
@@ -53,7 +53,7 @@ def test_certified_config1_sample_matches_gsl(engine):
     assert inverse_rel_err(inv, ir, batch.n, batch.offA) <= INV_TOL
 
 
-@pytest.mark.parametrize("lo,hi", [(33, 64), (65, 128), (129, 192), (193, 216)])
+@pytest.mark.parametrize("lo,hi", [(33, 64), (65, 128), (129, 192), (193, 224)])
 def test_certified_every_class_matches_gsl(engine, lo, hi):
     rng = np.random.default_rng(lo)
     sizes = list(range(lo, hi + 1, 3)) + [lo, hi]
@@ -68,12 +68,12 @@ def test_certified_every_class_matches_gsl(engine, lo, hi):
 
 # the streamed kernel: 64-column steps, so the orders around multiples of 64
 # (partial last tiles and steps) and both ends of its range
-STREAMED_ORDERS = [217, 230, 255, 256, 257, 300, 319, 320, 321, 383, 384, 449, 511, 512, 513, 640, 700, 777,
+STREAMED_ORDERS = [225, 230, 255, 256, 257, 300, 319, 320, 321, 383, 384, 449, 511, 512, 513, 640, 700, 777,
                    895, 960, 1000, 1023, 1024]
 
 
 def test_certified_streamed_orders_match_gsl(engine):
-    batch = wl.macro_batch(STREAMED_ORDERS, seed=217, density=0.10)
+    batch = wl.macro_batch(STREAMED_ORDERS, seed=225, density=0.10)
     inv, st, diag = run_plan(engine, batch, engine.FAST)
     ir, sr = ref_invert(batch)
     np.testing.assert_array_equal(st, sr)
@@ -87,7 +87,7 @@ def test_certified_streamed_fallback_and_odd_layout(engine):
     to SIROCCO_FP64); the good ones are inverted at offsets that leave their
     rows 8-byte but not 16-byte aligned (an odd number of doubles before each)."""
     rng = np.random.default_rng(23)
-    good = [wl.macro_matrix(rng, int(n), density=0.10) for n in (218, 260, 402, 514)]
+    good = [wl.macro_matrix(rng, int(n), density=0.10) for n in (226, 260, 402, 514)]
     bad = []
     m = wl.macro_matrix(rng, 300, density=0.10)
     m[17, 40] = 2e-3                            # a positive off-diagonal entry
@@ -164,7 +164,7 @@ def uncertified_matrices(rng):
 def test_uncertified_fall_back_to_the_exact_path(engine):
     rng = np.random.default_rng(11)
     bad = uncertified_matrices(rng)
-    good = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 217, 40)]
+    good = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 225, 40)]
     mats = good[:20] + bad + good[20:]
     batch = wl.from_matrices("invert", mats)
     inv, st, diag = run_plan(engine, batch, engine.FAST)
@@ -190,7 +190,7 @@ def test_uncertified_fall_back_to_the_exact_path(engine):
 def test_certified_plan_in_a_cuda_graph(engine):
     import torch
     rng = np.random.default_rng(5)
-    mats = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 217, 300)]
+    mats = [wl.macro_matrix(rng, int(n)) for n in rng.integers(33, 225, 300)]
     mats += [wl.macro_matrix(rng, int(n), density=0.10) for n in (230, 333, 480)]   # the streamed kernel's queue
     bad = uncertified_matrices(rng)
     batch = wl.from_matrices("invert", mats[:150] + bad + mats[150:])

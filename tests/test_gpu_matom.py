@@ -29,7 +29,7 @@ def reference_walk(row_b, z):
 def test_matom_matrices_match_inverse_times_r(engine, mode):
     """B equals the engine's own inverse in the same mode times R, bit for bit,
     and C its left-to-right running totals; in SIROCCO_FAST the certified
-    kernel forms both itself (orders 33-216 here), the GSL-exact path and the
+    kernel forms both itself (orders 33-224 here), the GSL-exact path and the
     epilogue kernel the rest."""
     m = getattr(engine, mode)
     batch, R, offv = wl.matom_cells(SIZES, seed=11)
