@@ -129,9 +129,11 @@ struct CgjShape {
   static constexpr int off_Dnext = off_Dinv + 8 * SP;   // [8][SP]
   static constexpr int buf = off_Dnext + 8 * SP;
   // R' has one buffer: S3 writes it after a step's first barrier and the last
-  // reader (S4 and the pivot warp) is done before the next step's first barrier
+  // reader (S4 and the pivot warp) is done before the next step's first barrier.
+  // A single row of tile warps (WGR = 1) keeps R' in registers instead.
+  static constexpr bool REGR = (WGR_ == 1);
   static constexpr int off_RowNT = 2 * buf;             // [P][SP]
-  static constexpr int off_dg = off_RowNT + SP * P;     // [LP] diagonal of each local row
+  static constexpr int off_dg = off_RowNT + (REGR ? 0 : SP * P);   // [LP] diagonal of each local row
   static constexpr int off_ok = off_dg + LP;            // [2][8] certificate of each CTA, by item parity
   static constexpr int off_bar = off_ok + 16;           // the staging mbarrier (8 bytes)
   static constexpr int SLOT = 8 * P + 2;                // doubles per staged 8-row block (+ alignment shift)
@@ -297,8 +299,11 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
             v1 = W[i][j][1];
           }
         const int r = grow(i);
-        ColP[lrow(i) * SP + 2 * t] = ((r == kb + 2 * t) ? 1.0 : 0.0) - v0;
-        ColP[lrow(i) * SP + 2 * t + 1] = ((r == kb + 2 * t + 1) ? 1.0 : 0.0) - v1;
+        // with R' in registers the columns are stored in slice order (column
+        // 2t + e at 4e + t, see S3)
+        const int p0 = S::REGR ? t : 2 * t, p1 = S::REGR ? 4 + t : 2 * t + 1;
+        ColP[lrow(i) * SP + p0] = ((r == kb + 2 * t) ? 1.0 : 0.0) - v0;
+        ColP[lrow(i) * SP + p1] = ((r == kb + 2 * t + 1) ? 1.0 : 0.0) - v1;
       }
     }
     if (kblk + 1 < NBLK) {
@@ -557,51 +562,98 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
         cluster_barrier<CL>();   // also orders the pivot warp's D^-1 of this block
       }
 
-      // S3: R' = D^-1 R outside K, I + D^-1 on K's columns; an 8-column block
-      // per warp at a time, two MMAs with D^-1 as the row operand
-      if (tile) {
-        const double a0 = Dinv[g * SP + t], a1 = Dinv[g * SP + 4 + t];
-        for (int cb = warp; cb < CBK; cb += NW) {
-          double d[2];
-          if (cb == kblk) {
-            d[0] = Dinv[g * SP + 2 * t] + ((g == 2 * t) ? 1.0 : 0.0);
-            d[1] = Dinv[g * SP + 2 * t + 1] + ((g == 2 * t + 1) ? 1.0 : 0.0);
-          } else {
-            const double b0 = RowPT[(cb * 8 + g) * SP + t], b1 = RowPT[(cb * 8 + g) * SP + 4 + t];
-            d[0] = 0.0;
-            d[1] = 0.0;
-            dmma_884(d, a0, b0);
-            dmma_884(d, a1, b1);
+      if constexpr (S::REGR) {
+        // S3 in registers: each tile warp forms R' (D^-1 R outside K, I + D^-1
+        // on K's columns) for its own columns, transposed (R'^T = R^T D^-T):
+        // the accumulator gives each lane R'[2t][c] and R'[2t + 1][c] of column
+        // c = 8 cb + g, the B operand of the update for the k-slices {2t} and
+        // {2t + 1}; the column panel is stored in that slice order.  No R'
+        // buffer, so no barrier between S3 and S4.
+        const double d0 = Dinv[g * SP + t], d1 = Dinv[g * SP + 4 + t];   // D^-T, B operand
+        if (tile) {
+          double bf[WC][2];
+#pragma unroll
+          for (int j = 0; j < WC; ++j) {
+            const int cb = wc + WGC * j;
+            if (cb == kblk) {
+              bf[j][0] = Dinv[(2 * t) * SP + g] + ((g == 2 * t) ? 1.0 : 0.0);
+              bf[j][1] = Dinv[(2 * t + 1) * SP + g] + ((g == 2 * t + 1) ? 1.0 : 0.0);
+            } else {
+              bf[j][0] = 0.0;
+              bf[j][1] = 0.0;
+              dmma_884(bf[j], RowPT[(cb * 8 + g) * SP + t], d0);
+              dmma_884(bf[j], RowPT[(cb * 8 + g) * SP + 4 + t], d1);
+            }
           }
-          RowNT[(cb * 8 + 2 * t) * SP + g] = d[0];
-          RowNT[(cb * 8 + 2 * t + 1) * SP + g] = d[1];
-        }
-      }
-      __syncthreads();
-
-      if (tile) {
-        // S4: W += (-C') R', two MMAs per sub-block
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          double a[WR], b[WC];
-#pragma unroll
-          for (int i = 0; i < WR; ++i) a[i] = ColP[lrow(i) * SP + 4 * h + t];
-#pragma unroll
-          for (int j = 0; j < WC; ++j) b[j] = RowNT[((wc + WGC * j) * 8 + g) * SP + 4 * h + t];
+          // S4: W += (-C') R', two MMAs per sub-block
 #pragma unroll
           for (int i = 0; i < WR; ++i)
 #pragma unroll
-            for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a[i], b[j]);
-        }
-      } else if (kblk + 1 < NBLK && rank == (kblk + 1) % CL) {
-        // the next pivot block, updated exactly as its holders update it, then inverted
-        const int lr0 = ((kblk + 1) / CL) * 8;
-        const double* Dn = B + S::off_Dnext;
-        double d[2] = {Dn[g * SP + 2 * t], Dn[g * SP + 2 * t + 1]};
+            for (int h = 0; h < 2; ++h) {
+              const double a = ColP[lrow(i) * SP + 4 * h + t];
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-          dmma_884(d, ColP[(lr0 + g) * SP + 4 * h + t], RowNT[(kb + 8 + g) * SP + 4 * h + t]);
-        pivot_inverse(kblk + 1, d[0], d[1]);
+              for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a, bf[j][h]);
+            }
+        } else if (kblk + 1 < NBLK && rank == (kblk + 1) % CL) {
+          // the next pivot block, updated exactly as its holder updates it
+          // (R' of its columns formed here), then inverted
+          const int lr0 = ((kblk + 1) / CL) * 8;
+          const double* Dn = B + S::off_Dnext;
+          double r1[2] = {0.0, 0.0};
+          dmma_884(r1, RowPT[((kblk + 1) * 8 + g) * SP + t], d0);
+          dmma_884(r1, RowPT[((kblk + 1) * 8 + g) * SP + 4 + t], d1);
+          double d[2] = {Dn[g * SP + 2 * t], Dn[g * SP + 2 * t + 1]};
+#pragma unroll
+          for (int h = 0; h < 2; ++h) dmma_884(d, ColP[(lr0 + g) * SP + 4 * h + t], r1[h]);
+          pivot_inverse(kblk + 1, d[0], d[1]);
+        }
+      } else {
+        // S3: R' = D^-1 R outside K, I + D^-1 on K's columns; an 8-column block
+        // per warp at a time, two MMAs with D^-1 as the row operand
+        if (tile) {
+          const double a0 = Dinv[g * SP + t], a1 = Dinv[g * SP + 4 + t];
+          for (int cb = warp; cb < CBK; cb += NW) {
+            double d[2];
+            if (cb == kblk) {
+              d[0] = Dinv[g * SP + 2 * t] + ((g == 2 * t) ? 1.0 : 0.0);
+              d[1] = Dinv[g * SP + 2 * t + 1] + ((g == 2 * t + 1) ? 1.0 : 0.0);
+            } else {
+              const double b0 = RowPT[(cb * 8 + g) * SP + t], b1 = RowPT[(cb * 8 + g) * SP + 4 + t];
+              d[0] = 0.0;
+              d[1] = 0.0;
+              dmma_884(d, a0, b0);
+              dmma_884(d, a1, b1);
+            }
+            RowNT[(cb * 8 + 2 * t) * SP + g] = d[0];
+            RowNT[(cb * 8 + 2 * t + 1) * SP + g] = d[1];
+          }
+        }
+        __syncthreads();
+
+        if (tile) {
+          // S4: W += (-C') R', two MMAs per sub-block
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            double a[WR], b[WC];
+#pragma unroll
+            for (int i = 0; i < WR; ++i) a[i] = ColP[lrow(i) * SP + 4 * h + t];
+#pragma unroll
+            for (int j = 0; j < WC; ++j) b[j] = RowNT[((wc + WGC * j) * 8 + g) * SP + 4 * h + t];
+#pragma unroll
+            for (int i = 0; i < WR; ++i)
+#pragma unroll
+              for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a[i], b[j]);
+          }
+        } else if (kblk + 1 < NBLK && rank == (kblk + 1) % CL) {
+          // the next pivot block, updated exactly as its holders update it, then inverted
+          const int lr0 = ((kblk + 1) / CL) * 8;
+          const double* Dn = B + S::off_Dnext;
+          double d[2] = {Dn[g * SP + 2 * t], Dn[g * SP + 2 * t + 1]};
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            dmma_884(d, ColP[(lr0 + g) * SP + 4 * h + t], RowNT[(kb + 8 + g) * SP + 4 * h + t]);
+          pivot_inverse(kblk + 1, d[0], d[1]);
+        }
       }
     }
 
