@@ -29,6 +29,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -92,7 +93,9 @@ def make_batches(config: int, nsys: int | None = None):
     raise SystemExit(f"unknown config {config}")
 
 
-CGJ_P = (40, 48, 56, 64, 80, 96, 112, 128, 144, 160, 176, 192, 208, 224)   # csrc/cgj_classes.inc
+# padded orders of the certified classes, as the engine compiles them in
+CGJ_P = tuple(int(m[1]) for m in re.finditer(r"^SS_CGJ_CLASS\(\d+, (\d+),",
+                                              (ROOT / "python_b200" / "csrc" / "cgj_classes.inc").read_text(), re.M))
 
 
 def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:

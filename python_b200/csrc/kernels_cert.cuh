@@ -44,25 +44,30 @@
 // 2(l%4) and 2(l%4)+1).  Each CTA also runs one pivot warp that holds no tile.
 // Every block step moves only the two panels through shared memory:
 //   S1  the warps holding K's rows write R (transposed, RowPT[c][q]) into
-//       their CTA's shared memory, where the other CTAs of a cluster read
-//       their S3 operands (distributed shared memory); the warps holding K's
-//       columns write
+//       the shared memory of every CTA of the cluster (remote stores into
+//       distributed shared memory, so that S3 reads are local); the warps
+//       holding K's columns write
 //       -C' (ColPN[r][q] = I - C on D's diagonal, -C elsewhere) locally; the
 //       holder of the next pivot block writes its current values (Dnext);
-//                                                               cluster barrier
-//   S3  the tile warps form R' = D^-1 R (RowNT[c][q]), two MMAs per 8-column
-//       block;                                                  barrier
+//       then a cluster barrier;
+//   S3  R' = D^-1 R, two MMAs per 8-column block: with a single row of tile
+//       warps (WGR = 1) each warp forms R' for its own columns in registers
+//       (computed transposed, so that the accumulator is already the update's
+//       B operand); otherwise the tile warps share the columns and write R'
+//       to shared memory (RowNT[c][q]), followed by a barrier;
 //   S4  every tile warp adds (-C') R' into each of its sub-blocks, two MMAs per
 //       sub-block from one operand load per row and per column block, while
 //       the pivot warp of the CTA that owns the next block brings Dnext up to
 //       date with the same MMAs in the same order and inverts it (8 x 8, the
 //       accumulator fragment's two entries per lane, shuffles), writing D^-1 of
 //       the next step into every CTA of the cluster.
-// So the serial 8 x 8 inverse overlaps the bulk update, and a step costs two
-// barriers.  Panel rows hold 8 values at a stride of SP = 12 doubles: the
-// operand fragments (8 panel rows x 4 values per load) then fall on distinct
-// banks.  The row panel, -C', D^-1 and Dnext are double-buffered by step
-// parity; R' needs one buffer.  B200's FP64 tensor-core MMA runs
+// So the serial 8 x 8 inverse overlaps the bulk update, and a step costs one
+// cluster barrier (plus one CTA barrier when R' goes through shared memory).
+// A matrix of order n takes ceil(n / 8) steps: the blocks beyond it hold only
+// the identity padding, which no step would change.  Panel rows hold 8 values
+// at a stride of SP = 12 doubles: the operand fragments (8 panel rows x 4
+// values per load) then fall on distinct banks.  The row panel, -C', D^-1 and
+// Dnext are double-buffered by step parity.  B200's FP64 tensor-core MMA runs
 // at the FP64 FMA rate (both ~37 TF/s here); it is used for its eight-fold
 // fewer issued instructions and its operand reuse across a warp, and it keeps
 // the FMA pipe free for the pivot warp's chain.
@@ -264,6 +269,9 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
   auto gcol = [&](int j, int e) -> int { return (wc + WGC * j) * 8 + 2 * t + e; };
   auto bufp = [&](int kblk) -> double* { return sm + (kblk & 1) * S::buf; };
   double W[WR][WC][2];
+  // block steps of the current matrix: those whose pivot block holds no row
+  // of it would only carry the identity padding along, so they are skipped
+  int nbe = NBLK;
 
   // S1 of block kblk: the old row panel, -C' and the next pivot block's values
   auto publish = [&](int kblk) {
@@ -285,6 +293,17 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
           }
         RowPT[gcol(j, 0) * SP + g] = v0;
         RowPT[gcol(j, 1) * SP + g] = v1;
+        if (CL > 1) {
+          // the row panel also goes straight into the other CTAs' shared memory,
+          // so that every CTA reads its S3 operands locally
+#pragma unroll
+          for (int pr = 0; pr < CL; ++pr) {
+            if (pr == rank) continue;
+            double* rp = cg::this_cluster().map_shared_rank(RowPT, pr);
+            rp[gcol(j, 0) * SP + g] = v0;
+            rp[gcol(j, 1) * SP + g] = v1;
+          }
+        }
       }
     }
     if (wc == kblk % WGC) {
@@ -306,7 +325,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
         ColP[lrow(i) * SP + p1] = ((r == kb + 2 * t + 1) ? 1.0 : 0.0) - v1;
       }
     }
-    if (kblk + 1 < NBLK) {
+    if (kblk + 1 < nbe) {
       const int k1 = kblk + 1, lbK1 = k1 / CL;
       if (rank == k1 % CL && wr == lbK1 % WGR && wc == k1 % WGC) {
         const int i1 = lbK1 / WGR, j1 = k1 / WGC;
@@ -411,6 +430,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
   for (int item = cid; item < cnt; item += ncl, parity ^= 1) {
     const int s = bv.list[item];
     const int n = bv.n[s];
+    nbe = (n + 7) / 8;
 
     // ---- this matrix's rows from the staging slots into registers (identity
     // padding), and the certificate's partial sums
@@ -545,13 +565,9 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
     cluster_barrier<CL>();
 
     // ---- blocked Gauss-Jordan, one 8 x 8 pivot block per step
-    for (int kblk = 0; kblk < NBLK; ++kblk) {
+    for (int kblk = 0; kblk < nbe; ++kblk) {
       double* B = bufp(kblk);
-      // the row panel lives in the shared memory of the CTA that owns block
-      // kblk; the other CTAs of a cluster read its operands from there
-      const double* RowPT = B + S::off_RowPT;
-      if (CL > 1 && rank != kblk % CL)
-        RowPT = cg::this_cluster().map_shared_rank(const_cast<double*>(RowPT), kblk % CL);
+      const double* RowPT = B + S::off_RowPT;   // written into every CTA by the owner
       double* RowNT = sm + S::off_RowNT;
       const double* ColP = B + S::off_ColP;
       const double* Dinv = B + S::off_Dinv;
@@ -594,7 +610,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
 #pragma unroll
               for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a, bf[j][h]);
             }
-        } else if (kblk + 1 < NBLK && rank == (kblk + 1) % CL) {
+        } else if (kblk + 1 < nbe && rank == (kblk + 1) % CL) {
           // the next pivot block, updated exactly as its holder updates it
           // (R' of its columns formed here), then inverted
           const int lr0 = ((kblk + 1) / CL) * 8;
@@ -644,7 +660,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
 #pragma unroll
               for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a[i], b[j]);
           }
-        } else if (kblk + 1 < NBLK && rank == (kblk + 1) % CL) {
+        } else if (kblk + 1 < nbe && rank == (kblk + 1) % CL) {
           // the next pivot block, updated exactly as its holders update it, then inverted
           const int lr0 = ((kblk + 1) / CL) * 8;
           const double* Dn = B + S::off_Dnext;
@@ -680,8 +696,8 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
       // a warp takes 32 local rows and walks them in 32 x 32 tiles, loaded and
       // stored coalesced through shared memory (the panel buffers, free now),
       // each lane adding its own row left to right as the reference does.
-      // A cluster barrier first: the other CTAs may still be reading this
-      // CTA's row panel, in these buffers, for their last step.
+      // A cluster barrier first: warps of this CTA may still be reading the
+      // last step's panels in these buffers.
       cluster_barrier<CL>();
       double* __restrict__ Cg = ep.C + bv.offA[s];
       constexpr int NG = (LP + 31) / 32;

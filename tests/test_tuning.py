@@ -35,3 +35,29 @@ def test_candidates_of_one_order_share_storage_and_chunk_width():
         by_p.setdefault(c[0], set()).add((c[5], c[3] if c[5] else None))
     for p, kinds in by_p.items():
         assert len(kinds) == 1, (p, kinds)
+
+
+def test_certified_class_table_comes_from_the_candidates():
+    """Every certified class is one of the tuner's candidate shapes, in order of P."""
+    cands = set(autotune.parse_cgj_candidates())
+    classes = autotune.parse_cgj_classes()
+    assert classes, "no certified classes"
+    assert [c[0] for c in classes] == sorted({c[0] for c in classes})
+    for c in classes:
+        assert c in cands, c
+
+
+def test_certified_record_matches_table():
+    """When the certified classes were tuned, the table is the record's winners
+    at the class edges the record kept."""
+    if not autotune.RECORD.exists():
+        return
+    rec = json.loads(autotune.RECORD.read_text()).get("cgj")
+    if rec is None:
+        return
+    chosen = {e["P"]: tuple(e["chosen"]) for e in rec["classes"]}
+    dropped = {e["P"] for e in rec["edges"] if e["dropped"]}
+    table = autotune.parse_cgj_classes()
+    assert sorted(set(chosen) - dropped) == [c[0] for c in table]
+    for c in table:
+        assert chosen[c[0]] == tuple(c), (chosen[c[0]], c)
