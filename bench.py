@@ -93,9 +93,15 @@ def make_batches(config: int, nsys: int | None = None):
     raise SystemExit(f"unknown config {config}")
 
 
-# padded orders of the certified classes, as the engine compiles them in
-CGJ_P = tuple(int(m[1]) for m in re.finditer(r"^SS_CGJ_CLASS\(\d+, (\d+),",
-                                              (ROOT / "python_b200" / "csrc" / "cgj_classes.inc").read_text(), re.M))
+# the engine's size classes, as it compiles them in (padded orders)
+def _class_orders(inc: str, macro: str) -> tuple:
+    text = (ROOT / "python_b200" / "csrc" / inc).read_text()
+    return tuple(int(m[1]) for m in re.finditer(rf"^{macro}\(\d+, (\d+),", text, re.M))
+
+
+CGJ_P = _class_orders("cgj_classes.inc", "SS_CGJ_CLASS")
+SMALL_NP = _class_orders("small_classes.inc", "SS_SMALL_CLASS")
+CTA_P = _class_orders("cta_classes.inc", "SS_CTA_CLASS")
 
 
 def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:
@@ -105,10 +111,10 @@ def size_class(n: int, kind: str = "solve", mode: str = "fp64") -> str:
             if n <= p:
                 return f"cgj{p}"
         return "cgjl"   # streamed certified inverse, orders above the last class
-    for np_ in (4, 8, 12, 16, 20, 24, 28, 32):
+    for np_ in SMALL_NP:
         if n <= np_:
             return f"small{np_}"
-    for p in (48, 64, 96, 128, 160, 192, 208, 224, 256, 320, 384, 448, 512, 640, 768, 896, 1024):
+    for p in CTA_P:
         if n <= p:
             return f"cta{p}"
     return "global"

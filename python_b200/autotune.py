@@ -18,9 +18,16 @@ then sets the class edges: from the top down, a class whose orders the next
 kept class's winner inverts faster is dropped.  It writes
 ``csrc/cgj_classes.inc``.
 
-Both write every timing into ``tuned_classes.json`` and rebuild the engine.
+``--family small``: the warp-group kernels of orders up to 32.  Each
+candidate of ``csrc/tune_small_candidates.inc`` (a padded row length NP and a
+lane count G >= NP per system) solves batches of ion-balance systems at two
+orders of its class; all candidates must return the same bits.  The fastest G
+per NP is kept, class edges are chosen as for the certified classes, and
+``csrc/small_classes.inc`` is written.
 
-    python -m python_b200.autotune [--family cgj]   # on a B200; then commit the written files
+All three write every timing into ``tuned_classes.json`` and rebuild the engine.
+
+    python -m python_b200.autotune [--family cgj|small]   # on a B200; then commit the written files
 """
 from __future__ import annotations
 
@@ -57,6 +64,11 @@ CGJ_BUILD = PKG / "_build" / "tune_cgj"
 CGJ_MIN_ORDER = 33               # below this the exact path's warp-group kernels serve certified inverses too
 CGJ_WORK_FLOP = 5.0e10           # floating-point work per timed launch (certified classes)
 CGJ_AGREE = 1e-12                # largest difference between two shapes' inverses, relative to the largest entry
+
+SMALL_CANDIDATES = CSRC / "tune_small_candidates.inc"
+SMALL_CLASS_INC = CSRC / "small_classes.inc"
+SMALL_TUNE_LIB = PKG / "_build" / "libsirocco_tune_small.so"
+SMALL_SYSTEMS = 1 << 18          # solves per timed launch (a generated set, repeated)
 
 
 def parse_candidates(path: Path = CANDIDATES):
@@ -137,8 +149,11 @@ def write_outputs(best: dict, record: dict) -> None:
         P, NT, RG, CC, PW, GM, MINB = best[p]
         lines.append(f"SS_CTA_CLASS({i}, {P}, {NT}, {RG}, {CC}, {PW}, {'true' if GM else 'false'}, {MINB})")
     CLASS_INC.write_text("\n".join(lines) + "\n")
-    if RECORD.exists() and "cgj" in (old := json.loads(RECORD.read_text())):
-        record["cgj"] = old["cgj"]   # the certified classes' record stays
+    if RECORD.exists():
+        old = json.loads(RECORD.read_text())
+        for key in ("cgj", "small"):   # the other families' records stay
+            if key in old:
+                record[key] = old[key]
     RECORD.write_text(json.dumps(record, indent=1) + "\n")
 
 
@@ -363,9 +378,166 @@ def tune_cgj(args) -> int:
     return 0
 
 
+# ------------------------------------------------------------- small systems --
+def parse_small_candidates(path: Path = SMALL_CANDIDATES):
+    return [(int(m[1]), int(m[2])) for m in re.finditer(r"^SS_TUNE_SMALL\((\d+), (\d+)\)", path.read_text(), re.M)]
+
+
+def parse_small_classes(path: Path = SMALL_CLASS_INC):
+    return [(int(m[1]), int(m[2])) for m in
+            re.finditer(r"^SS_SMALL_CLASS\(\d+, (\d+), (\d+)\)", path.read_text(), re.M)]
+
+
+def build_small_tune_lib() -> Path:
+    deps = [CSRC / "tune_small.cu", SMALL_CANDIDATES] + build.HEADERS
+    if build._stale(SMALL_TUNE_LIB, deps):
+        SMALL_TUNE_LIB.parent.mkdir(parents=True, exist_ok=True)
+        tmp = SMALL_TUNE_LIB.with_suffix(".so.tmp")
+        subprocess.run([build.NVCC, *build.ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                        "--expt-relaxed-constexpr", "-cudart", "static", "-o", str(tmp),
+                        str(CSRC / "tune_small.cu")], check=True, cwd=str(CSRC))
+        tmp.replace(SMALL_TUNE_LIB)
+    return SMALL_TUNE_LIB
+
+
+def load_small_lib():
+    lib = ctypes.CDLL(str(build_small_tune_lib()))
+    lib.sirocco_tune_info.argtypes = [c_int, POINTER(c_int)]
+    lib.sirocco_tune_time.argtypes = [c_int, c_int] + [c_void_p] * 9 + [c_int, POINTER(c_float), POINTER(c_int)]
+    cands = []
+    for i in range(lib.sirocco_tune_count()):
+        cfg = (c_int * 2)()
+        lib.sirocco_tune_info(i, cfg)
+        cands.append((i, (cfg[0], cfg[1])))
+    return lib, cands
+
+
+class _DeviceSolves:
+    """SMALL_SYSTEMS ion-balance solves of order n on the device: a generated
+    set of 4,096 systems, repeated."""
+
+    def __init__(self, n: int, device):
+        import torch
+        base = wl.ion_batch([n] * 4096, seed=3000 + n)
+        reps = SMALL_SYSTEMS // base.nsys
+        self.nsys = base.nsys * reps
+        self.flops = base.flops() * reps
+        a, b = base.A.size, base.b.size
+        self.n = torch.full((self.nsys,), n, dtype=torch.int32, device=device)
+        k = torch.arange(reps, dtype=torch.int64, device=device).repeat_interleave(base.nsys)
+        self.offA = torch.from_numpy(base.offA).to(device).repeat(reps) + k * a
+        self.offv = torch.from_numpy(base.offv).to(device).repeat(reps) + k * b
+        self.A = torch.from_numpy(base.A).to(device).repeat(reps)
+        self.b = torch.from_numpy(base.b).to(device).repeat(reps)
+        self.x = torch.empty_like(self.b)
+        self.st = torch.empty((self.nsys,), dtype=torch.int32, device=device)
+        self.list = torch.arange(self.nsys, dtype=torch.int32, device=device)
+
+
+def run_small(lib, i: int, ds: _DeviceSolves, reps: int):
+    import torch
+    ds.x.fill_(float("nan"))
+    ds.st.fill_(-99)
+    ms, res = c_float(), c_int()
+    rc = lib.sirocco_tune_time(i, ds.nsys, *(c_void_p(t.data_ptr()) for t in
+                                             (ds.n, ds.offA, ds.offv, ds.A, ds.b, ds.x, ds.st, ds.list)),
+                               reps, ctypes.byref(ms), ctypes.byref(res))
+    torch.cuda.synchronize()
+    if rc != 0:
+        return None, None, rc, 0
+    return ds.x.cpu().numpy(), ds.st.cpu().numpy(), ms.value, res.value
+
+
+def write_small_outputs(classes: list, notes: dict, record: dict) -> None:
+    lines = ["// Size classes of the small-system family (kernels_small.cuh, kernels_mixed.cuh).",
+             "// Written by `python -m python_b200.autotune --family small` from its timings on a",
+             "// B200 (every candidate of tune_small_candidates.inc; the record is",
+             "// python_b200/tuned_classes.json, key \"small\").",
+             "// SS_SMALL_CLASS(index, padded row length NP, lanes per system G)",
+             "// A system of order n <= NP runs on G >= NP lanes of a warp (lane r holds row r),",
+             "// 128 / G systems per CTA of 128 threads.  After each class: the winner's rate at",
+             "// the tuner's test orders."]
+    for i, (np_, g) in enumerate(classes):
+        lines.append(f"SS_SMALL_CLASS({i}, {np_}, {g})" + (f"  // {notes[np_]}" if np_ in notes else ""))
+    SMALL_CLASS_INC.write_text("\n".join(lines) + "\n")
+    old = json.loads(RECORD.read_text()) if RECORD.exists() else {}
+    old["small"] = record
+    RECORD.write_text(json.dumps(old, indent=1) + "\n")
+
+
+def tune_small(args) -> int:
+    import torch
+    dev = torch.device("cuda", 0)
+    lib, cands = load_small_lib()
+    orders = sorted({c[0] for _, c in cands})
+    record = {"device": torch.cuda.get_device_name(0), "when": datetime.datetime.now(datetime.timezone.utc).isoformat(),
+              "systems_per_launch": SMALL_SYSTEMS, "reps": args.reps, "classes": [], "edges": []}
+    win, scores, tests, cache = {}, {}, {}, {}
+
+    def solves(n):
+        if n not in cache:
+            cache.clear()
+            cache[n] = _DeviceSolves(n, dev)
+        return cache[n]
+
+    for k, np_ in enumerate(orders):
+        lo = orders[k - 1] + 1 if k else 2
+        tests[np_] = sorted({(lo + np_) // 2, np_})
+        mine = [(i, c) for i, c in cands if c[0] == np_]
+        entry = {"NP": np_, "orders": tests[np_], "candidates": []}
+        tot = {i: 0.0 for i, _ in mine}
+        for n in tests[np_]:
+            ds = solves(n)
+            ref = None
+            for i, cfg in mine:
+                x, st, ms, res = run_small(lib, i, ds, args.reps)
+                if x is None:
+                    raise SystemExit(f"candidate {cfg} failed to run: {ms}")
+                got = (x.tobytes(), st.tobytes())
+                if ref is None:
+                    ref = got
+                elif got != ref:
+                    raise SystemExit(f"candidate {cfg} disagrees with {mine[0][1]} at n={n}")
+                tot[i] += ms
+                entry["candidates"].append({"config": cfg, "n": n, "ms": ms, "ctas_per_sm": res,
+                                            "systems_per_s": ds.nsys / (ms * 1e-3)})
+        best = min(tot, key=tot.get)
+        win[np_] = (best, dict(mine)[best])
+        scores[np_] = tot[best]
+        entry["chosen"] = win[np_][1]
+        record["classes"].append(entry)
+        print(f"NP={np_:3d} orders {tests[np_]}: " + ", ".join(f"G={dict(mine)[i][1]}:{tot[i]:.3f}ms" for i in tot)
+              + f"  -> {win[np_][1]}", flush=True)
+
+    kept = [orders[-1]]
+    for np_ in reversed(orders[:-1]):
+        nxt = kept[0]
+        t_next = sum(run_small(lib, win[nxt][0], solves(n), args.reps)[2] for n in tests[np_])
+        drop = t_next < scores[np_]
+        record["edges"].append({"NP": np_, "next": nxt, "ms_own": scores[np_], "ms_next": t_next, "dropped": drop})
+        print(f"edge NP={np_}: own {scores[np_]:.3f} ms, by NP={nxt} {t_next:.3f} ms -> {'drop' if drop else 'keep'}",
+              flush=True)
+        if not drop:
+            kept.insert(0, np_)
+    classes = [win[np_][1] for np_ in kept]
+    notes = {}
+    for e in record["classes"]:
+        if e["NP"] in kept:
+            rates = [c["systems_per_s"] for c in e["candidates"] if tuple(c["config"]) == tuple(e["chosen"])]
+            notes[e["NP"]] = f"{min(rates) / 1e6:.0f}-{max(rates) / 1e6:.0f} M solves/s at orders {e['orders']}"
+    if args.dry_run:
+        print("classes:", classes)
+        return 0
+    write_small_outputs(classes, notes, record)
+    if not args.no_build:
+        build.build_engine(force=True)
+    print(f"wrote {SMALL_CLASS_INC.relative_to(PKG.parent)} and {RECORD.relative_to(PKG.parent)}")
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--family", choices=("cta", "cgj"), default="cta")
+    ap.add_argument("--family", choices=("cta", "cgj", "small"), default="cta")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--only", type=int, nargs="*", help="tune only these padded orders (others keep their entry)")
     ap.add_argument("--dry-run", action="store_true", help="time and print, write nothing")
@@ -373,6 +545,8 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     if args.family == "cgj":
         return tune_cgj(args)
+    if args.family == "small":
+        return tune_small(args)
     import torch
 
     lib, cands = load_tune_lib()

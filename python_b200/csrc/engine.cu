@@ -75,8 +75,14 @@ struct KernelSpec {
   int max_ctas = 0;        // CTAs resident on the whole GPU at once
 };
 
-// size classes of the small family (padded row length NP, lanes per system G)
-static const int kSmallNP[] = {4, 8, 12, 16, 20, 24, 28, 32};
+// size classes of the small family (padded row length NP; small_classes.inc,
+// chosen by python_b200/autotune.py --family small)
+static const int kSmallNP[] = {
+#define SS_SMALL_CLASS(I, NP, G) NP,
+#include "small_classes.inc"
+#undef SS_SMALL_CLASS
+};
+constexpr int kSmallClasses = int(sizeof(kSmallNP) / sizeof(kSmallNP[0]));
 // padded orders of the CTA classes (cta_classes.inc, chosen by python_b200/autotune.py)
 static const int kCtaP[] = {
 #define SS_CTA_CLASS(I, P, NT, RG, CC, PW, GM, MINB) P,
@@ -99,7 +105,7 @@ constexpr int kCgjMinN = 33;
 constexpr int kCgjlRT = 1, kCgjlMinB = 3;
 
 static int small_class(int n) {
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < kSmallClasses; ++i)
     if (n <= kSmallNP[i]) return i;
   return -1;
 }
@@ -119,7 +125,7 @@ template <int KIND>
 static KernelSpec small_spec(int cls, int mode) {
   KernelSpec k;
   k.threads = kSmallThreads;
-#define SS_SMALL(I, NP, G)                                                              \
+#define SS_SMALL_CLASS(I, NP, G)                                                        \
   case I:                                                                               \
     k.fn = (mode == SIROCCO_MIXED && KIND == kSolve)                                    \
                ? reinterpret_cast<const void*>(&small_mixed_solve_kernel<NP, G>)        \
@@ -127,17 +133,10 @@ static KernelSpec small_spec(int cls, int mode) {
     k.sys_per_block = kSmallThreads / G;                                                \
     break;
   switch (cls) {
-    SS_SMALL(0, 4, 4)
-    SS_SMALL(1, 8, 8)
-    SS_SMALL(2, 12, 16)
-    SS_SMALL(3, 16, 16)
-    SS_SMALL(4, 20, 32)
-    SS_SMALL(5, 24, 32)
-    SS_SMALL(6, 28, 32)
-    SS_SMALL(7, 32, 32)
+#include "small_classes.inc"
     default: break;
   }
-#undef SS_SMALL
+#undef SS_SMALL_CLASS
   return k;
 }
 
@@ -377,8 +376,8 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
   // Certified inverses (SIROCCO_FAST) go to the Gauss-Jordan classes; each also
   // has a place in the fallback list of its exact class (small or CTA family).
   const bool cert = (kind == kInvert && mode == SIROCCO_FAST);
-  std::vector<int> small_l[8], cta_l[kCtaClasses], glob_l, cgj_l[kCgjClasses], cgjl_l;
-  int small_fb[8] = {}, cta_fb[kCtaClasses] = {};
+  std::vector<int> small_l[kSmallClasses], cta_l[kCtaClasses], glob_l, cgj_l[kCgjClasses], cgjl_l;
+  int small_fb[kSmallClasses] = {}, cta_fb[kCtaClasses] = {};
   for (int s = 0; s < nsys; ++s) {
     const int ns = n[s];
     if (ns < 1 || ns > SIROCCO_MAX_N) {
@@ -405,7 +404,7 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
     else glob_l.push_back(s);
   }
   // fallback lists: one per exact class that certified systems belong to
-  int small_fbi[8], cta_fbi[kCtaClasses];
+  int small_fbi[kSmallClasses], cta_fbi[kCtaClasses];
   std::vector<int> xcls;
   if (cert) {
     int off = 0;
@@ -415,7 +414,7 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
       off += cnt;
       return p->nfb++;
     };
-    for (int e = 0; e < 8; ++e) small_fbi[e] = add_fb(small_fb[e]);
+    for (int e = 0; e < kSmallClasses; ++e) small_fbi[e] = add_fb(small_fb[e]);
     for (int e = 0; e < kCtaClasses; ++e) cta_fbi[e] = add_fb(cta_fb[e]);
     if (p->nfb > 0) {
       xcls.assign(nsys, -1);
@@ -483,12 +482,12 @@ static int plan_build(sirocco_plan** out, int kind, int nsys, const int* n, cons
     if ((rc = add_bucket(kFamCgj, c, cgj_l[c]))) return rc;
   for (int c = kCtaClasses - 1; c >= 0; --c)
     if ((rc = add_bucket(kFamCta, c, cta_l[c]))) return rc;
-  for (int c = 7; c >= 0; --c)
+  for (int c = kSmallClasses - 1; c >= 0; --c)
     if ((rc = add_bucket(kFamSmall, c, small_l[c]))) return rc;
   if (cert) {
     for (int c = kCtaClasses - 1; c >= 0; --c)
       if (cta_fbi[c] >= 0 && (rc = add_bucket_n(kFamCta, c, nullptr, cta_fbi[c], cta_fb[c]))) return rc;
-    for (int c = 7; c >= 0; --c)
+    for (int c = kSmallClasses - 1; c >= 0; --c)
       if (small_fbi[c] >= 0 && (rc = add_bucket_n(kFamSmall, c, nullptr, small_fbi[c], small_fb[c]))) return rc;
   }
 

@@ -61,3 +61,26 @@ def test_certified_record_matches_table():
     assert sorted(set(chosen) - dropped) == [c[0] for c in table]
     for c in table:
         assert chosen[c[0]] == tuple(c), (chosen[c[0]], c)
+
+
+def test_small_class_table_comes_from_the_candidates():
+    cands = set(autotune.parse_small_candidates())
+    classes = autotune.parse_small_classes()
+    assert classes and classes[-1][0] == 32, "orders up to 32 stay on the small family"
+    assert [c[0] for c in classes] == sorted({c[0] for c in classes})
+    for np_, g in classes:
+        assert (np_, g) in cands and np_ <= g and g in (4, 8, 16, 32)
+
+
+def test_small_record_matches_table():
+    if not autotune.RECORD.exists():
+        return
+    rec = json.loads(autotune.RECORD.read_text()).get("small")
+    if rec is None:
+        return
+    chosen = {e["NP"]: tuple(e["chosen"]) for e in rec["classes"]}
+    dropped = {e["NP"] for e in rec["edges"] if e["dropped"]}
+    table = autotune.parse_small_classes()
+    assert sorted(set(chosen) - dropped) == [c[0] for c in table]
+    for c in table:
+        assert chosen[c[0]] == tuple(c)
