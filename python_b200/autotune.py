@@ -403,7 +403,7 @@ def build_small_tune_lib() -> Path:
 def load_small_lib():
     lib = ctypes.CDLL(str(build_small_tune_lib()))
     lib.sirocco_tune_info.argtypes = [c_int, POINTER(c_int)]
-    lib.sirocco_tune_time.argtypes = [c_int, c_int] + [c_void_p] * 9 + [c_int, POINTER(c_float), POINTER(c_int)]
+    lib.sirocco_tune_time.argtypes = [c_int, c_int] + [c_void_p] * 8 + [c_int, POINTER(c_float), POINTER(c_int)]
     cands = []
     for i in range(lib.sirocco_tune_count()):
         cfg = (c_int * 2)()
