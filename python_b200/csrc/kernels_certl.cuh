@@ -146,6 +146,17 @@ __device__ __forceinline__ void store_acc(const Acc& acc, double* dst, int n, in
   }
 }
 
+// rows [r0, r0 + rb) x columns [c0, c0 + cb) of an n x n row-major matrix
+// brought into L2 (one prefetch per 16 doubles, every address inside the block)
+__device__ __forceinline__ void prefetch_l2(const double* src, int n, int r0, int rb, int c0, int cb, int tid,
+                                            int nth) {
+  const int lpr = (cb + 15) >> 4;
+  for (int e = tid; e < rb * lpr; e += nth) {
+    const int r = e / lpr, l = e - r * lpr;
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(src + int64_t(r0 + r) * n + c0 + 16 * l));
+  }
+}
+
 // acc += A B over the 64-deep tiles: warp (wr, wc) covers rows 32 wr .. +32,
 // columns 32 wc .. +32 in 4 x 4 fragments
 __device__ __forceinline__ void mma_tile(Acc& acc, const double* __restrict__ As, const double* __restrict__ Bs,
@@ -363,6 +374,33 @@ __global__ void __launch_bounds__(128 * RT, MINB)
           load_acc(acc, src, n, i0, ib, j0, jb, jt == kt || !act, vs, wr, wc, g, t);
           load_tile<NTH>(Bs, Wg, n, k0, kb, j0, jb, false, tid);
           __syncthreads();
+          // the next tile's operands (or the next pass's column strips and
+          // first tile) are brought into L2 while this tile's MMAs run
+          if (jt + 1 < nb) {
+            const int j1 = (jt + 1) * BT, jb1 = min(BT, n - j1);
+            prefetch_l2(Wg, n, k0, kb, j1, jb1, tid, NTH);
+            if (jt + 1 != kt) {
+#pragma unroll
+              for (int q = 0; q < RT; ++q) {
+                const int uq = ip + q;
+                if (uq < nb - 1) {
+                  const int iq = tile_row(uq) * BT;
+                  prefetch_l2(src, n, iq, min(BT, n - iq), j1, jb1, tid, NTH);
+                }
+              }
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < RT; ++q) {
+              const int uq = ip + RT + q;
+              if (uq < nb - 1) {
+                const int iq = tile_row(uq) * BT, ibq = min(BT, n - iq);
+                prefetch_l2(src, n, iq, ibq, k0, kb, tid, NTH);
+                if (kt != 0) prefetch_l2(src, n, iq, ibq, 0, min(BT, n), tid, NTH);
+              }
+            }
+            prefetch_l2(Wg, n, k0, kb, 0, min(BT, n), tid, NTH);
+          }
           if (act) {
             mma_any(acc, Ao, Bs, wr, wc, g, t, ib, jb, kb);
             store_acc(acc, Wg, n, i0, ib, j0, jb, Rs, vW, wr, wc, g, t);
