@@ -238,6 +238,9 @@ def ref_ion_rate_matrix(tab, rates, cell: int, xne: float, nh1: float, nh2: floa
 
 # ------------------------------------------------- macro-atom jump matrices --
 MATOM_LIB = HERE / "_ref" / "libref_matom.so"
+# the same reference routine with its invert_matrix resolved by the engine
+# (python_b200/libsirocco_solve.so) through the drop-in C ABI
+MATOM_DROPIN_LIB = HERE / "_ref" / "libref_matom_dropin.so"
 
 
 def matom_density_ratio(m, cell, density_phot_min: float = 1e-10):
@@ -363,10 +366,11 @@ def matom_reference_available() -> bool:
     return MATOM_LIB.exists()
 
 
-def ref_matom_b(m, cell, density_phot_min: float = 1e-10):
+def ref_matom_b(m, cell, density_phot_min: float = 1e-10, dropin: bool = False):
     """The reference's own calc_matom_matrix (oracle/_ref/libref_matom.so) on the
-    same model and coefficients: B = N^-1 diag(R), (nlev + 1)^2 row-major."""
-    lib = ctypes.CDLL(str(MATOM_LIB))
+    same model and coefficients: B = N^-1 diag(R), (nlev + 1)^2 row-major.  With
+    dropin, the build whose invert_matrix is the engine's (libref_matom_dropin.so)."""
+    lib = ctypes.CDLL(str(MATOM_DROPIN_LIB if dropin else MATOM_LIB))
     f = lib.refmatom_b
     f.restype = c_int
     i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)

@@ -54,6 +54,8 @@ def build_oracle(reference: bool = True) -> None:
             targets.append("refion")
         if (ref_tree / "source" / "macro_accelerate.c").exists():
             targets.append("refmatom")
+            if LIB.exists():
+                targets.append("refmatom_dropin")   # links the engine built above
         if (ref_tree / "source" / "matrix_gpu.cu").exists():
             targets.append("refgpu")
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), f"REF={ref_tree}", *targets], check=True)
