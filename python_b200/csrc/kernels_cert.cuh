@@ -274,13 +274,16 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
   int nbe = NBLK;
 
   // S1 of block kblk: the old row panel, -C' and the next pivot block's values
+  // REGR classes on a cluster push each row panel ahead (during the update of
+  // the step before), so publish then leaves it out
+  constexpr bool kEarlyRows = S::REGR && (CL > 1);
   auto publish = [&](int kblk) {
     double* B = bufp(kblk);
     double* RowPT = B + S::off_RowPT;
     double* ColP = B + S::off_ColP;
     const int kb = 8 * kblk;
     const int lbK = kblk / CL;
-    if (rank == kblk % CL && wr == lbK % WGR) {
+    if (!(kEarlyRows && kblk > 0) && rank == kblk % CL && wr == lbK % WGR) {
       const int iK = lbK / WGR;
 #pragma unroll
       for (int j = 0; j < WC; ++j) {
@@ -601,14 +604,43 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
               dmma_884(bf[j], RowPT[(cb * 8 + g) * SP + 4 + t], d1);
             }
           }
-          // S4: W += (-C') R', two MMAs per sub-block
+          // S4: W += (-C') R', two MMAs per sub-block.  On a cluster, the CTA
+          // holding the next row block updates that block first and pushes it
+          // as the next row panel into every CTA, so that the remote stores
+          // complete during the rest of the update rather than at the barrier
+          const bool early = kEarlyRows && kblk + 1 < nbe && rank == (kblk + 1) % CL;
+          const int iK1 = (kblk + 1) / CL;   // its local block (one row of tile warps)
+          if (early) {
+            double* RowN = bufp(kblk + 1) + S::off_RowPT;
+#pragma unroll
+            for (int i = 0; i < WR; ++i)
+              if (i == iK1) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                  const double a = ColP[lrow(i) * SP + 4 * h + t];
+#pragma unroll
+                  for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a, bf[j][h]);
+                }
+#pragma unroll
+                for (int j = 0; j < WC; ++j) {
+#pragma unroll
+                  for (int pr = 0; pr < CL; ++pr) {
+                    double* rp = (pr == rank) ? RowN : cg::this_cluster().map_shared_rank(RowN, pr);
+                    rp[gcol(j, 0) * SP + g] = W[i][j][0];
+                    rp[gcol(j, 1) * SP + g] = W[i][j][1];
+                  }
+                }
+              }
+          }
 #pragma unroll
           for (int i = 0; i < WR; ++i)
+            if (!(early && i == iK1)) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const double a = ColP[lrow(i) * SP + 4 * h + t];
+              for (int h = 0; h < 2; ++h) {
+                const double a = ColP[lrow(i) * SP + 4 * h + t];
 #pragma unroll
-              for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a, bf[j][h]);
+                for (int j = 0; j < WC; ++j) dmma_884(W[i][j], a, bf[j][h]);
+              }
             }
         } else if (kblk + 1 < nbe && rank == (kblk + 1) % CL) {
           // the next pivot block, updated exactly as its holder updates it
