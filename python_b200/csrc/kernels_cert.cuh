@@ -14,8 +14,12 @@
 //     reference returns code 0 (lu.c:540 `singular` never fires) and the only
 //     question is accuracy.
 // The certificate checked per matrix, on the FP64 input, is
-//     a_rr > 0,  a_rc <= 0 (c != r),  sum_{c != r} |a_rc| * (1 + 2^-40) <= (1 - tau) a_rr
-// for every row r, tau = kCertMargin, with every entry finite.  Measured against
+//     1/4 <= a_rr <= 4,  a_rc <= 0 (c != r),  sum_{c != r} |a_rc| * (1 + 2^-40) <= (1 - tau) a_rr
+// for every row r, tau = kCertMargin, with every entry finite.  The bound on
+// the diagonal is the fused update's (below): it adds I to D^-1 and takes it
+// from the column panel, which is accurate relative to unit scale only; a row
+// scaled by 2^e loses about e bits (rows at 2^+-20: 2.7e-10 from the true
+// inverse), so matrices of other scales take the exact path.  Measured against
 // the reference's GSL inverse on M-matrices whose every row sits at the margin,
 // the no-pivot result differs by <= 4e-12 (relative, max-abs) at tau = 1e-5 and
 // grows like 1/tau below it; macro-atom matrices with realistic deactivation
@@ -59,8 +63,9 @@
 //       sub-block from one operand load per row and per column block, while
 //       the pivot warp of the CTA that owns the next block brings Dnext up to
 //       date with the same MMAs in the same order and inverts it (8 x 8, the
-//       accumulator fragment's two entries per lane, shuffles), writing D^-1 of
-//       the next step into every CTA of the cluster.
+//       accumulator fragment's two entries per lane, shuffles; on one-CTA
+//       classes an FP32 elimination refined by FP64 Newton steps), writing
+//       D^-1 of the next step into every CTA of the cluster.
 // So the serial 8 x 8 inverse overlaps the bulk update, and a step costs one
 // cluster barrier (plus one CTA barrier when R' goes through shared memory).
 // A matrix of order n takes ceil(n / 8) steps: the blocks beyond it hold only
@@ -86,6 +91,7 @@
 namespace ss {
 
 constexpr double kCertMargin = 1.0e-5;   // relative row-dominance margin of the certificate
+constexpr double kCertDiagLo = 0.25, kCertDiagHi = 4.0;   // the certificate's range of a_rr
 
 // Fallback lists of the certified launches: systems that fail the certificate
 // are appended, per exact-path size class, for the GSL-exact kernels.
@@ -147,7 +153,7 @@ struct CgjShape {
   static constexpr size_t dyn_smem = size_t(n_dbl) * 8;
   static_assert(P % (8 * CL) == 0 && LB % WGR == 0 && CBK % WGC == 0, "whole sub-block tiles");
   static_assert(NTH <= 1024, "one CTA");
-  static_assert(WGC * LP <= 2 * buf, "certificate partials fit the panel buffers");
+  static_assert(WGC * LP <= off_Dinv, "certificate partials leave D^-1 and Dnext free (pivot scratch)");
   static_assert(CL >= 1 && CL <= 8, "portable cluster sizes");
   static_assert(off_stage % 2 == 0 && SLOT % 2 == 0, "16-byte aligned staging slots");
   static_assert(buf % 2 == 0 && off_dg % 2 == 0, "16-byte aligned buffers");
@@ -241,6 +247,103 @@ __device__ __forceinline__ void warp_inv8(double& d0, double& d1, int lane) {
       d0 = fma(-f, nk0, (2 * h == k) ? 0.0 : d0);
       d1 = fma(-f, nk1, (2 * h + 1 == k) ? 0.0 : d1);
     }
+  }
+}
+
+// The same elimination in FP32, with the hardware's approximate reciprocal:
+// a starting point for warp_inv8_refined, on the FP32 pipe.
+__device__ __forceinline__ void warp_inv8_f32(float& d0, float& d1, int lane) {
+  const int q = lane >> 2, h = lane & 3;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int kh = k >> 1;
+    const float colv = (k & 1) ? d1 : d0;
+    const float dkk = __shfl_sync(0xffffffffu, colv, 4 * k + kh);
+    const float f = __shfl_sync(0xffffffffu, colv, 4 * q + kh);
+    const float rk0 = __shfl_sync(0xffffffffu, d0, 4 * k + h);
+    const float rk1 = __shfl_sync(0xffffffffu, d1, 4 * k + h);
+    float piv;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(piv) : "f"(dkk));
+    const float nk0 = (2 * h == k) ? piv : rk0 * piv;
+    const float nk1 = (2 * h + 1 == k) ? piv : rk1 * piv;
+    if (q == k) {
+      d0 = nk0;
+      d1 = nk1;
+    } else {
+      d0 = fmaf(-f, nk0, (2 * h == k) ? 0.0f : d0);
+      d1 = fmaf(-f, nk1, (2 * h + 1 == k) ? 0.0f : d1);
+    }
+  }
+}
+
+// |x| as the ordered high word of a double (sign cleared; NaN and Inf above
+// every finite value), for warp-wide maxima on the integer pipe
+__device__ __forceinline__ unsigned abs_hi(double x) {
+  return unsigned(__double2hiint(x)) & 0x7fffffffu;
+}
+__device__ __forceinline__ double neg_bits(double x) {   // -x by its sign bit
+  return __longlong_as_double(__double_as_longlong(x) ^ (1ll << 63));
+}
+
+// The 8 x 8 inverse of warp_inv8 with little FP64 work on its serial path: the
+// FP32 elimination above gives X, then Newton steps X <- X + X (I - D X) in
+// FP64 on the tensor cores (two MMAs for the residual, two for the update)
+// until the residual's largest entry is below 2^-27, after which the last
+// update leaves X at FP64 rounding.  A block whose first residual is 1/4 or
+// more (a badly conditioned or badly scaled D, an FP32 overflow, NaN) or that
+// has not converged after four steps is inverted by warp_inv8 instead.  Where
+// the pivot warp's chain is a step's critical path while the tile warps keep
+// the FP64 pipe busy, this moves all but ~12 of its ~64 FP64 instructions to
+// the FP32 pipe.  scrD and scrX are two free 8 x SP panels of
+// shared memory (row-major, stride SP) for the operand transposes.
+template <int SP>
+__device__ __forceinline__ void warp_inv8_refined(double& d0, double& d1, int lane, double* scrD,
+                                                  double* scrX) {
+  const int g = lane >> 2, t = lane & 3;
+  constexpr unsigned kHiQuarter = 1021u << 20;    // |e| >= 2^-2
+  constexpr unsigned kHiConverged = 996u << 20;   // |e| <  2^-27
+  float f0 = __double2float_rn(d0), f1 = __double2float_rn(d1);
+  warp_inv8_f32(f0, f1, lane);
+  double x0 = double(f0), x1 = double(f1);
+  __syncwarp();   // earlier reads of the scratch panels by this warp
+  scrD[g * SP + 2 * t] = neg_bits(d0);
+  scrD[g * SP + 2 * t + 1] = neg_bits(d1);
+  __syncwarp();
+  const double na0 = scrD[g * SP + t], na1 = scrD[g * SP + 4 + t];   // -D, A operand
+  bool ok = false;
+#pragma unroll 1
+  for (int it = 0; it < 4; ++it) {
+    scrX[g * SP + 2 * t] = x0;
+    scrX[g * SP + 2 * t + 1] = x1;
+    __syncwarp();
+    const double xb0 = scrX[t * SP + g], xb1 = scrX[(4 + t) * SP + g];   // X, B operand
+    const double xa0 = scrX[g * SP + t], xa1 = scrX[g * SP + 4 + t];     // X, A operand
+    __syncwarp();
+    double e[2] = {(g == 2 * t) ? 1.0 : 0.0, (g == 2 * t + 1) ? 1.0 : 0.0};
+    dmma_884(e, na0, xb0);
+    dmma_884(e, na1, xb1);
+    const unsigned em = __reduce_max_sync(0xffffffffu, max(abs_hi(e[0]), abs_hi(e[1])));
+    if (em >= kHiQuarter) break;
+    scrX[g * SP + 2 * t] = e[0];
+    scrX[g * SP + 2 * t + 1] = e[1];
+    __syncwarp();
+    const double eb0 = scrX[t * SP + g], eb1 = scrX[(4 + t) * SP + g];   // E, B operand
+    __syncwarp();
+    double xn[2] = {x0, x1};
+    dmma_884(xn, xa0, eb0);
+    dmma_884(xn, xa1, eb1);
+    x0 = xn[0];
+    x1 = xn[1];
+    if (em < kHiConverged) {
+      ok = true;
+      break;
+    }
+  }
+  if (ok) {
+    d0 = x0;
+    d1 = x1;
+  } else {
+    warp_inv8(d0, d1, lane);
   }
 }
 
@@ -350,7 +453,15 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
   // the pivot warp: D^-1 of block kblk from the 8 x 8 values d0, d1
   // (accumulator layout), written into every CTA's buffer of that block
   auto pivot_inverse = [&](int kblk, double d0, double d1) {
-    warp_inv8(d0, d1, lane);
+    // One CTA per matrix: the FP32 start and FP64 Newton steps (orders 57-64
+    // +15 %, 121-128 +5 %); on a cluster the FP64 elimination, which measured
+    // 0-5 % faster there.  Scratch: this block's D^-1 panel (written last) and
+    // the other buffer's Dnext panel (read by this warp already; rewritten two
+    // steps later)
+    if constexpr (CL == 1)
+      warp_inv8_refined<SP>(d0, d1, lane, bufp(kblk + 1) + S::off_Dnext, bufp(kblk) + S::off_Dinv);
+    else
+      warp_inv8(d0, d1, lane);
     double* Dinv = bufp(kblk) + S::off_Dinv;
     Dinv[g * SP + 2 * t] = d0;
     Dinv[g * SP + 2 * t + 1] = d1;
@@ -521,7 +632,7 @@ cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
       double off = 0.0;
       for (int q = 0; q < WGC; ++q) off += red[q * LP + lr];
       const double d = dg[lr];
-      rok &= (d > 0.0) && (d < INFINITY) && (off * (1.0 + 0x1p-40) <= (1.0 - kCertMargin) * d);
+      rok &= (d >= kCertDiagLo) && (d <= kCertDiagHi) && (off * (1.0 + 0x1p-40) <= (1.0 - kCertMargin) * d);
     }
     const int cert_cta = __syncthreads_and(int(zok && rok));
     const int stall_cta = __syncthreads_or(int(stalled));

@@ -4,7 +4,8 @@
 //
 // The certificate and the reason no pivoting is needed are those of
 // kernels_cert.cuh (nonsingular M-matrices with a relative row-dominance margin
-// of kCertMargin; the macro-atom matrices of calc_matom_matrix,
+// of kCertMargin and diagonal entries within [kCertDiagLo, kCertDiagHi]; the
+// macro-atom matrices of calc_matom_matrix,
 // source/macro_accelerate.c:268-284, inverted at :315).  A matrix that fails
 // it is appended to the fallback list of its GSL-exact class.
 //
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(128 * RT, MINB)
         }
       }
       off = warp_sum(off);
-      ok &= (d > 0.0) && (d < INFINITY) && (off * (1.0 + 0x1p-40) <= (1.0 - kCertMargin) * d);
+      ok &= (d >= kCertDiagLo) && (d <= kCertDiagHi) && (off * (1.0 + 0x1p-40) <= (1.0 - kCertMargin) * d);
     }
     if (!__syncthreads_and(int(ok))) {
       if (tid == 0) {

@@ -1,7 +1,8 @@
 """Certified inverses (SIROCCO_FAST) against the reference's GSL inverse.
 
 Matrices that pass the certificate (nonsingular M-matrices with a relative
-row-dominance margin of at least 1e-5) are inverted by Gauss-Jordan without
+row-dominance margin of at least 1e-5 and diagonal entries within [1/4, 4])
+are inverted by Gauss-Jordan without
 pivoting: code 0, as GSL's, and the inverse within 1e-10 (max-abs, relative to
 the largest entry) of the reference build's.  Orders 33-224 run the
 register-resident kernel, orders 225-1024 the streamed one.  Every other
@@ -130,6 +131,64 @@ def test_certified_config3_macro_sample(engine):
     ir, sr = ref_invert(batch)
     np.testing.assert_array_equal(st, sr)
     assert per_system_err(inv, ir, batch).max() <= INV_TOL
+
+
+def margin_matrix(rng, n, tau):
+    """A dense M-matrix whose every row sits just inside the certificate's
+    margin: unit diagonal, off-diagonal row sums 1 - tau (condition ~1/tau)."""
+    off = rng.uniform(0.0, 1.0, (n, n))
+    np.fill_diagonal(off, 0.0)
+    off *= (1.0 - tau) / off.sum(axis=1, keepdims=True)
+    return np.eye(n) - off
+
+
+@pytest.mark.parametrize("tau", [1.5e-5, 1e-3])
+def test_certified_pivot_blocks_near_the_margin(engine, tau):
+    # the one-CTA classes invert each 8 x 8 pivot block in FP32 and refine it
+    # by FP64 Newton steps; near the margin the late blocks are ill-conditioned
+    # enough to need more steps or the FP64 elimination instead
+    rng = np.random.default_rng(int(1 / tau))
+    sizes = [33, 40, 47, 56, 61, 64, 72, 90, 104, 119, 128, 150, 200]
+    batch = wl.from_matrices("invert", [margin_matrix(rng, n, tau) for n in sizes])
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    assert (diag == CERTIFIED_DIAG).all()
+    err = per_system_err(inv, ir, batch)
+    assert err.max() <= INV_TOL, (batch.n[np.argmax(err)], err.max())
+
+
+def test_certified_diagonal_scale(engine):
+    # The fused update adds I to each pivot block's inverse, which is accurate
+    # relative to unit scale only: the certificate takes diagonals in [1/4, 4]
+    # and leaves every other scale (rows at 2^+-150, whose FP32 pivot start
+    # would also overflow or underflow; a whole matrix times 8 or 1/8) to the
+    # exact path, bit-equal to SIROCCO_FP64.  Rows scaled within the range stay
+    # certified and within 1e-10 of GSL.
+    rng = np.random.default_rng(150)
+    mats, want_fb = [], []
+    for n in (37, 64, 100, 128, 170, 300):
+        mats.append(np.ldexp(1.0, rng.choice([-150, 0, 150], n))[:, None] * wl.macro_matrix(rng, n))
+        want_fb.append(True)
+    for n, f in ((45, 8.0), (90, 0.125), (200, 8.0)):
+        mats.append(f * wl.macro_matrix(rng, n))
+        want_fb.append(True)
+    for n in (40, 61, 120, 150, 260):
+        mats.append(np.ldexp(1.0, rng.choice([-2, -1, 0, 1, 2], n))[:, None] * wl.macro_matrix(rng, n))
+        want_fb.append(False)
+    batch = wl.from_matrices("invert", mats)
+    inv, st, diag = run_plan(engine, batch, engine.FAST)
+    inv64, st64, _ = run_plan(engine, batch, engine.FP64)
+    ir, sr = ref_invert(batch)
+    np.testing.assert_array_equal(st, sr)
+    np.testing.assert_array_equal(st, st64)
+    fb = (diag & (1 << 8)) != 0
+    assert fb.tolist() == want_fb, diag
+    for k in np.nonzero(fb)[0]:
+        o, n = int(batch.offA[k]), int(batch.n[k])
+        assert same_values(inv[o:o + n * n], inv64[o:o + n * n]).all(), n
+    err = per_system_err(inv, ir, batch)
+    assert err[~fb].max() <= INV_TOL, (batch.n[~fb], err[~fb])
 
 
 def uncertified_matrices(rng):
