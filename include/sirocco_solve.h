@@ -65,9 +65,10 @@ int gpu_invert_matrix(double *matrix, double *inverse, int num_rows);
                             exact FP64 for any system whose result or code the
                             refinement cannot vouch for                          */
 #define SIROCCO_FAST 2   /* inverses of certified matrices -- nonsingular
-                            M-matrices: positive diagonal, off-diagonal entries
-                            <= 0, every row strictly dominant by a relative
-                            margin of at least 1e-5, as the macro-atom jumping
+                            M-matrices: diagonal entries within [1/4, 4],
+                            off-diagonal entries <= 0, every row strictly
+                            dominant by a relative margin of at least 1e-5,
+                            as the macro-atom jumping
                             matrix N = I - Q/Q_norm is wherever every level can
                             deactivate -- by FP64 Gauss-Jordan without pivoting
                             (code 0, as GSL's, and within ~1e-11 of GSL's
