@@ -144,9 +144,9 @@ def margin_matrix(rng, n, tau):
 
 @pytest.mark.parametrize("tau", [1.5e-5, 1e-3])
 def test_certified_pivot_blocks_near_the_margin(engine, tau):
-    # the one-CTA classes invert each 8 x 8 pivot block in FP32 and refine it
-    # by FP64 Newton steps; near the margin the late blocks are ill-conditioned
-    # enough to need more steps or the FP64 elimination instead
+    # condition ~1e5 at tau = 1.5e-5; the one-CTA classes invert each 8 x 8
+    # pivot block in FP32 and refine it by FP64 Newton steps, the clusters by
+    # FP64 elimination
     rng = np.random.default_rng(int(1 / tau))
     sizes = [33, 40, 47, 56, 61, 64, 72, 90, 104, 119, 128, 150, 200]
     batch = wl.from_matrices("invert", [margin_matrix(rng, n, tau) for n in sizes])
