@@ -351,7 +351,7 @@ template <int P, int WGR, int WGC, int CL, int MINB, bool STAGE = true>
 __global__ void __launch_bounds__(32 * WGR * WGC + 32, MINB)
 cgj_inverse_kernel(BatchView bv, CertArgs ca, CertEpi ep) {
   using S = CgjShape<P, WGR, WGC, CL, MINB, STAGE>;
-  constexpr int NW = S::NW, NT = S::NT, WR = S::WR, WC = S::WC, LP = S::LP, LB = S::LB, CBK = S::CBK;
+  constexpr int NW = S::NW, WR = S::WR, WC = S::WC, LP = S::LP, LB = S::LB, CBK = S::CBK;
   constexpr int SP = S::SP, NBLK = P / 8;
   extern __shared__ __align__(16) double sm[];
   namespace cg = cooperative_groups;
